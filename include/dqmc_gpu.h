@@ -1,0 +1,168 @@
+/*
+ * dqmc_gpu.h -- C ABI of the B200 determinant-QMC engine (libdqmc_b200.so).
+ *
+ * The engine replaces the reference's sweep engine seam, the `Dqmc` API that
+ * dqmc_run_replica consumes (SAI-QMC src/dqmc.h:91-108, used at
+ * src/replica_run.c:124-126, 184-186, 284-453), with a batched engine: many
+ * independent chains (replicas x temperatures, uneven n and L) advance
+ * together on one GPU.  Plain pointers and sizes only; every matrix is
+ * n x n column-major (the reference's layout, src/linalg.h:4).
+ *
+ * Return convention (as the reference's dqmc_init_modes, src/dqmc.c:418):
+ * 0 = ok, nonzero = failure; dqmc_last_error() describes the last failure
+ * of the calling thread.  A chain whose numerics break is frozen with a
+ * nonzero status (src/dqmc.h:79-81 semantics: later sweeps are no-ops) and
+ * the other chains continue.  Calls on one engine are not thread-safe.
+ */
+#ifndef DQMC_GPU_H
+#define DQMC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DQMC_GPU_ABI_VERSION 1
+
+typedef struct dqmc_engine dqmc_engine;
+
+enum { DQMC_PREC_FP64 = 0, DQMC_PREC_MIXED = 1 };
+enum { DQMC_DRIFT_STAB = 1, DQMC_DRIFT_SCRATCH = 2 };
+
+/* Per-bin scalar layout returned by dqmc_read_bins (src/replica.h:6-16). */
+enum {
+    DQMC_BIN_SUM_SIGN_EHUB = 0,
+    DQMC_BIN_SUM_SIGN_EGC,
+    DQMC_BIN_SUM_SIGN_EPH,
+    DQMC_BIN_SUM_SIGN_N,
+    DQMC_BIN_SUM_SIGN_D,
+    DQMC_BIN_SUM_SIGN,
+    DQMC_BIN_COUNT_F,
+    DQMC_BIN_ACCEPTED_F,
+    DQMC_BIN_ATTEMPTS_F,
+    DQMC_BIN_NFIELDS
+};
+
+typedef struct {
+    int device;      /* CUDA device ordinal                                  */
+    int precision;   /* DQMC_PREC_*                                          */
+    int delay_rank;  /* site-block size k of the delayed update; 0 = by n    */
+    int drift;       /* bit-or of DQMC_DRIFT_*: STAB = max|G_wrap - G_stab|
+                        at every stabilization (on by default); SCRATCH =
+                        also the reference's rebuild-from-scratch drift
+                        (src/dqmc.c:64-98, costly)                            */
+    int reserved[8];
+} dqmc_engine_desc;
+
+typedef struct {
+    unsigned long long attempts;   /* src/dqmc.h:84-86 counters */
+    unsigned long long accepted;
+    unsigned long long sweeps;
+    int status;                    /* 0 healthy, else DQMC_ST_* bits */
+    int pad;
+    double sign;
+    double drift_max, drift_mean;  /* max|G_wrapped - G_stabilized|  */
+    unsigned long long drift_samples;
+    double scratch_drift_max, scratch_drift_mean;  /* reference drift */
+    unsigned long long scratch_drift_samples;
+    uint64_t rng[4];               /* xoshiro256** state (src/rng.h:6-8) */
+} dqmc_chain_counters;
+
+/* Fills a descriptor with the defaults (device 0, FP64, k by n, STAB drift). */
+void dqmc_desc_default(dqmc_engine_desc *desc);
+
+/* Creates an engine on desc->device.  Replaces the per-chain allocation of
+ * dqmc_init_modes (src/dqmc.c:418-483) for a whole batch. */
+dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc);
+void dqmc_engine_destroy(dqmc_engine *e);              /* src/dqmc.c:525-542 */
+const char *dqmc_last_error(void);
+
+/* Registers a Hubbard model on a lattice: hopping t (n x n), bipartite signs
+ * (+/-1), U, dtau, mu = U/2.  expK = exp(-dtau (t - mu)) and its inverse are
+ * computed on the host (model_init, src/model.c:8-31).  Lx, Ly give site
+ * coordinates i = x + Lx*y for the spin structure factors (0 if none).
+ * Returns the model id (>= 0) or -1. */
+int dqmc_model_add(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
+                   const int *bipart, double U, double dtau);
+
+/* Enables Szz(q) / Sperp(q) on a model for the q lists (mx, my), the
+ * structure_factor_plan_init selectors of src/structure_factor.c:107-206.
+ * nq = 0 disables a channel. */
+int dqmc_model_set_spin(dqmc_engine *e, int model, int nq_zz, const int *mx_zz,
+                        const int *my_zz, int nq_perp, const int *mx_perp,
+                        const int *my_perp);
+
+/* Adds a chain: L time slices, stabilization interval stab, seed of its
+ * xoshiro256** stream.  field == NULL draws the field from the stream
+ * exactly as field_init (src/field.c:18-23), consuming n*L uniforms; a
+ * non-NULL field (L x n, +/-1, slice-major s[l*n+i]) is used as given (the
+ * stream still advances by n*L).  Returns the chain id or -1. */
+int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
+                   const signed char *field);
+
+/* Allocates device state for all chains, uploads models and fields and
+ * builds each chain's G from scratch (green_from_scratch, src/green.c:262).
+ * nbin measurement bins are reserved per chain. */
+int dqmc_engine_prepare(dqmc_engine *e, int nbin);
+
+/* Advances every healthy chain by nsweeps forward sweeps (dqmc_sweep,
+ * src/dqmc.c:952-963).  Asynchronous; see dqmc_synchronize. */
+int dqmc_sweep(dqmc_engine *e, int nsweeps);
+
+/* As dqmc_sweep, and after each sweep measures every chain (measure_sample,
+ * src/measure.c:6-39; measure_szz_sperp_sample, src/structure_factor.c:
+ * 328-400) and accumulates the sign-weighted sample into bin `bin`
+ * (replica_result_add_sample, src/replica.c:240-269). */
+int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin);
+
+/* Waits for queued work; returns nonzero on a CUDA error. */
+int dqmc_synchronize(dqmc_engine *e);
+
+int dqmc_chain_count(const dqmc_engine *e);
+int dqmc_chain_dims(const dqmc_engine *e, int chain, int *n, int *L);
+
+/* Copies back the up-spin G (n x n) at the chain's current slice (0 after a
+ * sweep).  G_down = I - P G_up^T P (src/green.c:372-382). */
+int dqmc_read_green(dqmc_engine *e, int chain, double *G);
+int dqmc_read_field(dqmc_engine *e, int chain, signed char *field);
+/* Replaces a chain's field and rebuilds its G from scratch. */
+int dqmc_write_field(dqmc_engine *e, int chain, const signed char *field);
+int dqmc_read_counters(dqmc_engine *e, int chain, dqmc_chain_counters *out);
+
+/* Copies back the bin accumulators: scalars nbin x DQMC_BIN_NFIELDS,
+ * szz nbin x nq_zz, sperp nbin x nq_perp (either may be NULL). */
+int dqmc_read_bins(dqmc_engine *e, int chain, double *scalars, double *szz,
+                   double *sperp);
+/* Per-phase SM cycle counters of a chain (the reference's PROF regions,
+ * src/profiler.h:6-39, as device clocks): bcache, stack, propose, flush,
+ * wrap, bblock, lmul, combine, green, scratch-drift, adopt, measure.
+ * Copies min(count, 12) values. */
+int dqmc_read_profile(dqmc_engine *e, int chain, unsigned long long *cycles,
+                      int count);
+/* Clears all bins of all chains. */
+int dqmc_clear_bins(dqmc_engine *e);
+
+/* Test entry points (oracle parity).  They return nonzero only on an API or
+ * CUDA error; a numerical breakdown is reported as *det_sign == 0. */
+/* G from scratch at slice l0 for a chain's current field, without touching
+ * the chain (green_from_scratch, src/green.c:262-306). */
+int dqmc_green_from_scratch(dqmc_engine *e, int chain, int l0, double *G,
+                            int *det_sign);
+/* One wrap G <- B_l G B_l^{-1} of a caller G with the chain's field
+ * (green_wrap, src/green.c:509-527). */
+int dqmc_wrap_green(dqmc_engine *e, int chain, int l, double *G);
+/* G = (1 + U diag(D) T)^{-1} and sign det(1 + U D T) on the device for a
+ * caller UDV (udv_inv_one_plus_work, src/linalg.c:911-1115; D signed as in
+ * the reference). */
+int dqmc_udv_green(int device, int n, const double *U, const double *D,
+                   const double *T, double *G, int *det_sign);
+
+/* Host helper: out = exp(scale * A) for symmetric A (la_expm_sym,
+ * src/linalg.c:319-346). */
+int dqmc_expm_sym(int n, const double *A, double scale, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,95 @@
+/* Device-side data layout shared by the host engine and the kernels.
+ *
+ * Every matrix is n x n, column-major, leading dimension n (the reference's
+ * layout, linalg.h:4).  One chain's device state lives in one contiguous
+ * arena (see dqmc_engine.cu, chain_arena_layout) so a chain is one pointer
+ * plus offsets; chains of different (n, L) coexist in one launch.
+ */
+#pragma once
+#include <stdint.h>
+
+#define DQMC_NT 256          /* threads per CTA; one CTA owns one chain   */
+#define DQMC_MAX_N 1024      /* largest lattice the kernels are laid out for */
+#define DQMC_MAX_KB 64       /* largest site block of the delayed update    */
+#define DQMC_QNB 16          /* Householder panel width                     */
+
+/* status bits (per chain, sticky; a chain with status != 0 is frozen)     */
+#define DQMC_ST_NONFINITE 1  /* non-finite value in a factor or in G        */
+#define DQMC_ST_SINGULAR 2   /* zero pivot in a QR                          */
+#define DQMC_ST_LOGRANGE 4   /* log-scale D left the representable range   */
+#define DQMC_ST_DETSIGN 8    /* det sign came out 0                         */
+
+/* per-bin scalar accumulators (replica.h:6-16 ReplicaBin order)           */
+enum {
+    DQMC_BIN_EHUB = 0,
+    DQMC_BIN_EGC,
+    DQMC_BIN_EPH,
+    DQMC_BIN_N,
+    DQMC_BIN_D,
+    DQMC_BIN_SIGN,
+    DQMC_BIN_COUNT,
+    DQMC_BIN_ACCEPTED,
+    DQMC_BIN_ATTEMPTS,
+    DQMC_BIN_FIELDS
+};
+
+/* phase timers (SM clock cycles, thread 0, phases are barrier-separated) */
+enum {
+    DQMC_PH_BCACHE = 0,   /* B-block products for the suffix stack (first sweep) */
+    DQMC_PH_STACK,        /* suffix stack rmuls                                  */
+    DQMC_PH_PROPOSE,      /* site-block proposals (warp 0) incl. block loads     */
+    DQMC_PH_FLUSH,        /* rank-m flush of the accepted block                  */
+    DQMC_PH_WRAP,         /* G <- B G B^-1                                       */
+    DQMC_PH_BBLOCK,       /* left B-block products                               */
+    DQMC_PH_LMUL,         /* left UDV update                                     */
+    DQMC_PH_COMBINE,      /* left x suffix                                       */
+    DQMC_PH_GREEN,        /* (1 + UDT)^-1                                        */
+    DQMC_PH_SDRIFT,       /* reference drift rebuild (opt-in)                    */
+    DQMC_PH_ADOPT,        /* drift + copy of the stabilized G                    */
+    DQMC_PH_MEASURE,      /* fused measurement                                   */
+    DQMC_PH_COUNT
+};
+
+typedef struct {
+    int n, Lx, Ly;
+    double U, dtau, mu;
+    double expv[2];     /* exp(+lambda*s - dtau*U/2) for s = -1, +1 (green.c:63-67) */
+    double expvinv[2];  /* 1/expv                                           */
+    double Nup[2];      /* N_cache[sigma=+1][s] = exp(-2 lambda s) - 1 (field.c:11-17) */
+    double Ndn[2];      /* N_cache[sigma=-1][s] = exp(+2 lambda s) - 1      */
+    const double *expK, *expKinv, *thop;
+    const int *bipart;
+    int nq_zz, nq_perp;
+    const double *cos_zz, *cos_perp;   /* n x nq phase tables (structure_factor.c:182-199) */
+} DqmcModelDev;
+
+typedef struct {
+    int model, n, L, stab, M, kb;
+    int status, bvalid;        /* bvalid: cached B-block products are current */
+    double sign;
+    unsigned long long attempts, accepted, sweeps;
+    unsigned long long meas_accepted, meas_attempts;  /* counters at last measurement */
+    uint64_t rng[4];
+    /* drift: max|G_wrapped - G_stabilized| over stabilization points       */
+    double drift_max, drift_sum;
+    unsigned long long drift_count;
+    /* reference-style drift (rebuild from scratch), opt-in                 */
+    double sdrift_max, sdrift_sum;
+    unsigned long long sdrift_count;
+    /* arena pointers */
+    signed char *field;        /* L x n */
+    double *G;                 /* n x n */
+    double *S;                 /* (M+1) UDV slots */
+    double *left, *comb, *scr; /* UDV slots (scr: rebuilds from scratch) */
+    double *bcache;            /* M x n x n block products B(b_{j+1}, b_j) */
+    double *w[6];              /* n x n scratch */
+    double *Zs, *Ys;           /* n x kb flush operands */
+    double *twall;             /* n x QNB compact-WY factors of the last QR */
+    double *bins;              /* nbin x DQMC_BIN_FIELDS */
+    double *bins_zz, *bins_perp;   /* nbin x nq */
+    int nbin;
+    unsigned long long prof[DQMC_PH_COUNT];
+} DqmcChainDev;
+
+/* UDV slot: U (n*n) | T (n*n) | ell = log D (n) | detU (1) | pad (1)        */
+#define DQMC_UDV_SIZE(n) (2 * (size_t)(n) * (n) + (size_t)(n) + 2)

@@ -1,0 +1,728 @@
+/* Host side of libdqmc_b200: the C ABI declared in include/dqmc_gpu.h.
+ *
+ * Owns device memory (one arena per engine: every chain's state is a slice
+ * of it), the stream, and the launches.  Setup work that the reference does
+ * per replica on the host (model_init's matrix exponential, rng_seed,
+ * field_init) stays on the host here too; everything per sweep runs on the
+ * device.  There is no CPU fallback: without a CUDA device every call that
+ * needs one fails with an error.
+ */
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dqmc_gpu.h"
+#include "dqmc_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return 1;
+}
+
+#define CU(call)                                                                 \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess)                                                   \
+            return set_err("%s failed: %s", #call, cudaGetErrorString(e_));      \
+    } while (0)
+
+/* splitmix64 seeding and xoshiro256** (src/rng.c:8-37), host copy used for
+ * field_init before the stream moves to the device. */
+uint64_t splitmix(uint64_t *x)
+{
+    uint64_t z = (*x += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+double host_rng_next(uint64_t *s)
+{
+    const uint64_t res = ((s[1] * 5) << 7 | (s[1] * 5) >> 57) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = (s[3] << 45) | (s[3] >> 19);
+    return (double)(res >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/* Symmetric eigendecomposition by cyclic Jacobi rotations; A is overwritten
+ * by its eigenvalues on the diagonal, V receives the eigenvectors. */
+void jacobi_eig(int n, std::vector<double> &a, std::vector<double> &V)
+{
+    V.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) V[i + (size_t)i * n] = 1.0;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int j = 0; j < n; ++j) {
+            diag += a[j + (size_t)j * n] * a[j + (size_t)j * n];
+            for (int i = 0; i < j; ++i) off += a[i + (size_t)j * n] * a[i + (size_t)j * n];
+        }
+        if (off <= 1e-34 * (diag + 1e-300)) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = a[p + (size_t)q * n];
+                if (apq == 0.0) continue;
+                const double app = a[p + (size_t)p * n], aqq = a[q + (size_t)q * n];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double tt = (theta >= 0 ? 1.0 : -1.0) /
+                                  (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(tt * tt + 1.0), s = tt * c;
+                for (int k = 0; k < n; ++k) {
+                    double &akp = a[k + (size_t)p * n], &akq = a[k + (size_t)q * n];
+                    const double x = akp, y = akq;
+                    akp = c * x - s * y;
+                    akq = s * x + c * y;
+                }
+                for (int k = 0; k < n; ++k) {
+                    double &apk = a[p + (size_t)k * n], &aqk = a[q + (size_t)k * n];
+                    const double x = apk, y = aqk;
+                    apk = c * x - s * y;
+                    aqk = s * x + c * y;
+                }
+                for (int k = 0; k < n; ++k) {
+                    double &vkp = V[k + (size_t)p * n], &vkq = V[k + (size_t)q * n];
+                    const double x = vkp, y = vkq;
+                    vkp = c * x - s * y;
+                    vkq = s * x + c * y;
+                }
+            }
+    }
+}
+
+size_t rup(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct HModel {
+    int n, Lx, Ly;
+    double U, dtau;
+    std::vector<double> thop, expK, expKinv, cos_zz, cos_perp;
+    std::vector<int> bipart;
+    int nq_zz = 0, nq_perp = 0;
+};
+
+struct HChain {
+    int model, L, stab, M, kb;
+    uint64_t rng[4];
+    std::vector<signed char> field;
+};
+
+}  // namespace
+
+struct dqmc_engine {
+    dqmc_engine_desc desc;
+    std::vector<HModel> models;
+    std::vector<HChain> chains;
+    cudaStream_t stream = nullptr;
+    char *dmod = nullptr, *darena = nullptr;
+    DqmcModelDev *dmodels = nullptr;
+    DqmcChainDev *dchains = nullptr;
+    std::vector<DqmcChainDev> hdev;  /* host mirror: device pointers */
+    int nbin = 0;
+    size_t smem = 0, msmem = 0;
+    bool prepared = false;
+};
+
+extern "C" {
+
+const char *dqmc_last_error(void) { return g_err.c_str(); }
+
+void dqmc_desc_default(dqmc_engine_desc *d)
+{
+    std::memset(d, 0, sizeof *d);
+    d->device = 0;
+    d->precision = DQMC_PREC_FP64;
+    d->delay_rank = 0;
+    d->drift = DQMC_DRIFT_STAB;
+}
+
+int dqmc_expm_sym(int n, const double *A, double scale, double *out)
+{
+    if (n <= 0 || !A || !out) return set_err("dqmc_expm_sym: bad arguments");
+    std::vector<double> a(A, A + (size_t)n * n), V;
+    jacobi_eig(n, a, V);
+    std::vector<double> f(n);
+    for (int k = 0; k < n; ++k) f[k] = std::exp(scale * a[k + (size_t)k * n]);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int k = 0; k < n; ++k) s += V[i + (size_t)k * n] * f[k] * V[j + (size_t)k * n];
+            out[i + (size_t)j * n] = s;
+        }
+    return 0;
+}
+
+dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
+{
+    dqmc_engine_desc d;
+    if (desc)
+        d = *desc;
+    else
+        dqmc_desc_default(&d);
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        set_err("no CUDA device available (%s); the engine has no CPU path",
+                e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+        return nullptr;
+    }
+    if (d.device < 0 || d.device >= ndev) {
+        set_err("device %d out of range (%d devices)", d.device, ndev);
+        return nullptr;
+    }
+    if (cudaSetDevice(d.device) != cudaSuccess) {
+        set_err("cudaSetDevice(%d) failed", d.device);
+        return nullptr;
+    }
+    dqmc_engine *eng = new dqmc_engine();
+    eng->desc = d;
+    if (cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_err("cudaStreamCreate failed");
+        delete eng;
+        return nullptr;
+    }
+    return eng;
+}
+
+void dqmc_engine_destroy(dqmc_engine *e)
+{
+    if (!e) return;
+    cudaSetDevice(e->desc.device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    cudaFree(e->dmod);
+    cudaFree(e->darena);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int dqmc_model_add(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
+                   const int *bipart, double U, double dtau)
+{
+    if (!e || e->prepared) return -set_err("dqmc_model_add: engine missing or prepared");
+    if (n <= 0 || n > DQMC_MAX_N || !thop || !bipart)
+        return -set_err("dqmc_model_add: n=%d outside 1..%d or null input", n, DQMC_MAX_N);
+    if (!(dtau > 0.0) || !(U >= 0.0)) return -set_err("dqmc_model_add: need U>=0, dtau>0");
+    HModel m;
+    m.n = n;
+    m.Lx = Lx;
+    m.Ly = Ly;
+    m.U = U;
+    m.dtau = dtau;
+    m.thop.assign(thop, thop + (size_t)n * n);
+    m.bipart.assign(bipart, bipart + n);
+    /* model_init (src/model.c:8-31): K = t - mu I with mu = U/2 */
+    std::vector<double> K(m.thop);
+    for (int i = 0; i < n; ++i) K[i + (size_t)i * n] -= U / 2.0;
+    m.expK.resize((size_t)n * n);
+    m.expKinv.resize((size_t)n * n);
+    dqmc_expm_sym(n, K.data(), -dtau, m.expK.data());
+    dqmc_expm_sym(n, K.data(), dtau, m.expKinv.data());
+    e->models.push_back(std::move(m));
+    return (int)e->models.size() - 1;
+}
+
+int dqmc_model_set_spin(dqmc_engine *e, int model, int nq_zz, const int *mx_zz,
+                        const int *my_zz, int nq_perp, const int *mx_perp,
+                        const int *my_perp)
+{
+    if (!e || e->prepared || model < 0 || model >= (int)e->models.size())
+        return set_err("dqmc_model_set_spin: bad engine/model");
+    HModel &m = e->models[model];
+    if ((nq_zz > 0 || nq_perp > 0) && (m.Lx <= 0 || m.Ly <= 0 || m.Lx * m.Ly != m.n))
+        return set_err("dqmc_model_set_spin: model has no site coordinates");
+    /* phase table of structure_factor_plan_init (src/structure_factor.c:
+     * 182-199): cos(2 pi (mx dx / Lx + my dy / Ly)) */
+    const double two_pi = 2.0 * std::acos(-1.0);
+    auto table = [&](int nq, const int *mx, const int *my, std::vector<double> &out) {
+        out.assign((size_t)m.n * nq, 0.0);
+        for (int q = 0; q < nq; ++q)
+            for (int d = 0; d < m.n; ++d) {
+                const int dx = d % m.Lx, dy = d / m.Lx;
+                const double ang = two_pi * ((double)mx[q] * (double)dx / (double)m.Lx +
+                                             (double)my[q] * (double)dy / (double)m.Ly);
+                out[d + (size_t)q * m.n] = std::cos(ang);
+            }
+    };
+    m.nq_zz = nq_zz > 0 ? nq_zz : 0;
+    m.nq_perp = nq_perp > 0 ? nq_perp : 0;
+    if (m.nq_zz) table(nq_zz, mx_zz, my_zz, m.cos_zz);
+    if (m.nq_perp) table(nq_perp, mx_perp, my_perp, m.cos_perp);
+    return 0;
+}
+
+int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
+                   const signed char *field)
+{
+    if (!e || e->prepared || model < 0 || model >= (int)e->models.size())
+        return -set_err("dqmc_chain_add: bad engine/model");
+    if (L <= 0) return -set_err("dqmc_chain_add: L must be > 0");
+    const int n = e->models[model].n;
+    HChain c;
+    c.model = model;
+    c.L = L;
+    c.stab = stab > 0 ? stab : 8;   /* green_stack_alloc default, src/green.c:172 */
+    c.M = (L + c.stab - 1) / c.stab;
+    int kb = e->desc.delay_rank;
+    if (kb <= 0) kb = n <= 256 ? 32 : 64;
+    if (kb > DQMC_MAX_KB) kb = DQMC_MAX_KB;
+    if (kb > n) kb = n;
+    c.kb = kb;
+    uint64_t x = seed;
+    for (int i = 0; i < 4; ++i) c.rng[i] = splitmix(&x);
+    c.field.resize((size_t)L * n);
+    /* field_init (src/field.c:18-23): one uniform per (l, i), always drawn */
+    for (size_t k = 0; k < c.field.size(); ++k)
+        c.field[k] = host_rng_next(c.rng) < 0.5 ? -1 : 1;
+    if (field) {
+        for (size_t k = 0; k < c.field.size(); ++k) {
+            if (field[k] != 1 && field[k] != -1)
+                return -set_err("dqmc_chain_add: field entries must be +/-1");
+            c.field[k] = field[k];
+        }
+    }
+    e->chains.push_back(std::move(c));
+    return (int)e->chains.size() - 1;
+}
+
+int dqmc_engine_prepare(dqmc_engine *e, int nbin)
+{
+    if (!e || e->prepared) return set_err("dqmc_engine_prepare: engine missing or prepared");
+    if (e->chains.empty()) return set_err("dqmc_engine_prepare: no chains");
+    CU(cudaSetDevice(e->desc.device));
+    e->nbin = nbin > 0 ? nbin : 1;
+    /* models */
+    size_t moff = 0;
+    std::vector<size_t> mo(e->models.size() * 6);
+    for (size_t k = 0; k < e->models.size(); ++k) {
+        const HModel &m = e->models[k];
+        const size_t nn = (size_t)m.n * m.n;
+        mo[6 * k + 0] = moff; moff += rup(nn * 8);
+        mo[6 * k + 1] = moff; moff += rup(nn * 8);
+        mo[6 * k + 2] = moff; moff += rup(nn * 8);
+        mo[6 * k + 3] = moff; moff += rup((size_t)m.n * 4);
+        mo[6 * k + 4] = moff; moff += rup(m.cos_zz.size() * 8 + 8);
+        mo[6 * k + 5] = moff; moff += rup(m.cos_perp.size() * 8 + 8);
+    }
+    const size_t mstruct = moff;
+    moff += rup(sizeof(DqmcModelDev) * e->models.size());
+    CU(cudaMalloc(&e->dmod, moff));
+    std::vector<DqmcModelDev> hm(e->models.size());
+    for (size_t k = 0; k < e->models.size(); ++k) {
+        const HModel &m = e->models[k];
+        const size_t nn = (size_t)m.n * m.n;
+        DqmcModelDev &d = hm[k];
+        std::memset(&d, 0, sizeof d);
+        d.n = m.n;
+        d.Lx = m.Lx;
+        d.Ly = m.Ly;
+        d.U = m.U;
+        d.dtau = m.dtau;
+        d.mu = m.U / 2.0;
+        /* field.c:10-17, green.c:63-67 (sigma = +1 for the evolved spin) */
+        const double lambda = std::acosh(std::exp(m.dtau * m.U / 2.0));
+        const double c = -m.dtau * m.U / 2.0;
+        d.expv[0] = std::exp(lambda * -1.0 + c);
+        d.expv[1] = std::exp(lambda * 1.0 + c);
+        d.expvinv[0] = 1.0 / d.expv[0];
+        d.expvinv[1] = 1.0 / d.expv[1];
+        for (int is = 0; is < 2; ++is) {
+            const double sv = is ? 1.0 : -1.0;
+            d.Nup[is] = std::exp(-2.0 * lambda * 1.0 * sv) - 1.0;
+            d.Ndn[is] = std::exp(-2.0 * lambda * -1.0 * sv) - 1.0;
+        }
+        d.expK = (const double *)(e->dmod + mo[6 * k + 0]);
+        d.expKinv = (const double *)(e->dmod + mo[6 * k + 1]);
+        d.thop = (const double *)(e->dmod + mo[6 * k + 2]);
+        d.bipart = (const int *)(e->dmod + mo[6 * k + 3]);
+        d.cos_zz = (const double *)(e->dmod + mo[6 * k + 4]);
+        d.cos_perp = (const double *)(e->dmod + mo[6 * k + 5]);
+        d.nq_zz = m.nq_zz;
+        d.nq_perp = m.nq_perp;
+        CU(cudaMemcpy(e->dmod + mo[6 * k + 0], m.expK.data(), nn * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->dmod + mo[6 * k + 1], m.expKinv.data(), nn * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->dmod + mo[6 * k + 2], m.thop.data(), nn * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->dmod + mo[6 * k + 3], m.bipart.data(), (size_t)m.n * 4,
+                      cudaMemcpyHostToDevice));
+        if (m.nq_zz)
+            CU(cudaMemcpy(e->dmod + mo[6 * k + 4], m.cos_zz.data(), m.cos_zz.size() * 8,
+                          cudaMemcpyHostToDevice));
+        if (m.nq_perp)
+            CU(cudaMemcpy(e->dmod + mo[6 * k + 5], m.cos_perp.data(), m.cos_perp.size() * 8,
+                          cudaMemcpyHostToDevice));
+    }
+    e->dmodels = (DqmcModelDev *)(e->dmod + mstruct);
+    CU(cudaMemcpy(e->dmodels, hm.data(), sizeof(DqmcModelDev) * hm.size(),
+                  cudaMemcpyHostToDevice));
+
+    /* chain arena layout */
+    const size_t nc = e->chains.size();
+    std::vector<size_t> base(nc);
+    size_t off = 0;
+    size_t maxsmem = 0;
+    int maxn = 0;
+    for (size_t k = 0; k < nc; ++k) {
+        const HChain &c = e->chains[k];
+        const HModel &m = e->models[c.model];
+        const int n = m.n;
+        const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
+        base[k] = off;
+        off += rup((size_t)c.L * n);                          /* field */
+        off += rup(nn * 8);                                   /* G */
+        off += rup((size_t)(c.M + 1) * usz * 8);              /* S */
+        off += 3 * rup(usz * 8);                              /* left, comb, scr */
+        off += rup((size_t)c.M * nn * 8);                     /* bcache */
+        off += 6 * rup(nn * 8);                               /* w */
+        off += 2 * rup((size_t)n * c.kb * 8);                 /* Zs, Ys */
+        off += rup((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB * DQMC_QNB * 8);
+        off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
+        off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
+        off += rup((size_t)e->nbin * m.nq_perp * 8 + 8);
+        const size_t sm = dq::smem_doubles(n, c.kb) * 8;
+        if (sm > maxsmem) maxsmem = sm;
+        if (n > maxn) maxn = n;
+    }
+    const size_t cstruct = off;
+    off += rup(sizeof(DqmcChainDev) * nc);
+    CU(cudaMalloc(&e->darena, off));
+    CU(cudaMemset(e->darena, 0, off));
+    e->hdev.assign(nc, DqmcChainDev());
+    for (size_t k = 0; k < nc; ++k) {
+        const HChain &c = e->chains[k];
+        const HModel &m = e->models[c.model];
+        const int n = m.n;
+        const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
+        DqmcChainDev &d = e->hdev[k];
+        std::memset(&d, 0, sizeof d);
+        d.model = c.model;
+        d.n = n;
+        d.L = c.L;
+        d.stab = c.stab;
+        d.M = c.M;
+        d.kb = c.kb;
+        d.nbin = e->nbin;
+        for (int i = 0; i < 4; ++i) d.rng[i] = c.rng[i];
+        char *p = e->darena + base[k];
+        auto take = [&](size_t bytes) { char *q = p; p += rup(bytes); return q; };
+        d.field = (signed char *)take((size_t)c.L * n);
+        d.G = (double *)take(nn * 8);
+        d.S = (double *)take((size_t)(c.M + 1) * usz * 8);
+        d.left = (double *)take(usz * 8);
+        d.comb = (double *)take(usz * 8);
+        d.scr = (double *)take(usz * 8);
+        d.bcache = (double *)take((size_t)c.M * nn * 8);
+        for (int i = 0; i < 6; ++i) d.w[i] = (double *)take(nn * 8);
+        d.Zs = (double *)take((size_t)n * c.kb * 8);
+        d.Ys = (double *)take((size_t)n * c.kb * 8);
+        d.twall = (double *)take((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB *
+                                 DQMC_QNB * 8);
+        d.bins = (double *)take((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
+        d.bins_zz = (double *)take((size_t)e->nbin * m.nq_zz * 8 + 8);
+        d.bins_perp = (double *)take((size_t)e->nbin * m.nq_perp * 8 + 8);
+        CU(cudaMemcpy(d.field, c.field.data(), c.field.size(), cudaMemcpyHostToDevice));
+    }
+    e->dchains = (DqmcChainDev *)(e->darena + cstruct);
+    CU(cudaMemcpy(e->dchains, e->hdev.data(), sizeof(DqmcChainDev) * nc,
+                  cudaMemcpyHostToDevice));
+    e->smem = maxsmem;
+    e->msmem = (size_t)2 * maxn * 8;
+    if (e->smem > 227 * 1024) return set_err("shared memory need %zu B exceeds 227 KB", e->smem);
+    CU(cudaFuncSetAttribute(dq::k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)e->smem));
+    CU(cudaFuncSetAttribute(dq::k_init, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)e->smem));
+    CU(cudaFuncSetAttribute(dq::k_scratch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)e->smem));
+    CU(cudaFuncSetAttribute(dq::k_wrap, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)e->smem));
+    CU(cudaFuncSetAttribute(dq::k_measure, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)e->msmem));
+    dq::k_init<<<(unsigned)nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(e->stream));
+    e->prepared = true;
+    return 0;
+}
+
+static int check_prepared(dqmc_engine *e, const char *who)
+{
+    if (!e || !e->prepared) return set_err("%s: engine not prepared", who);
+    if (cudaSetDevice(e->desc.device) != cudaSuccess) return set_err("%s: cudaSetDevice", who);
+    return 0;
+}
+
+static int kflags(const dqmc_engine *e)
+{
+    return (e->desc.drift & DQMC_DRIFT_SCRATCH) ? dq::KF_SDRIFT : 0;
+}
+
+int dqmc_sweep(dqmc_engine *e, int nsweeps)
+{
+    if (check_prepared(e, "dqmc_sweep")) return 1;
+    if (nsweeps <= 0) return 0;
+    dq::k_sweep<<<(unsigned)e->chains.size(), DQMC_NT, e->smem, e->stream>>>(
+        e->dchains, e->dmodels, kflags(e), nsweeps);
+    CU(cudaGetLastError());
+    return 0;
+}
+
+int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
+{
+    if (check_prepared(e, "dqmc_sweep_measure")) return 1;
+    if (bin < 0 || bin >= e->nbin) return set_err("dqmc_sweep_measure: bin %d out of range", bin);
+    const unsigned nc = (unsigned)e->chains.size();
+    for (int s = 0; s < nsweeps; ++s) {
+        dq::k_sweep<<<nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels,
+                                                         kflags(e) | dq::KF_MEASURE, 1);
+        dq::k_measure<<<nc, DQMC_NT, e->msmem, e->stream>>>(e->dchains, e->dmodels, bin);
+    }
+    CU(cudaGetLastError());
+    return 0;
+}
+
+int dqmc_synchronize(dqmc_engine *e)
+{
+    if (!e) return set_err("dqmc_synchronize: null engine");
+    CU(cudaSetDevice(e->desc.device));
+    CU(cudaStreamSynchronize(e->stream));
+    return 0;
+}
+
+int dqmc_chain_count(const dqmc_engine *e) { return e ? (int)e->chains.size() : 0; }
+
+int dqmc_chain_dims(const dqmc_engine *e, int chain, int *n, int *L)
+{
+    if (!e || chain < 0 || chain >= (int)e->chains.size()) return set_err("bad chain");
+    if (n) *n = e->models[e->chains[chain].model].n;
+    if (L) *L = e->chains[chain].L;
+    return 0;
+}
+
+static int chain_ok(dqmc_engine *e, int chain, const char *who)
+{
+    if (check_prepared(e, who)) return 1;
+    if (chain < 0 || chain >= (int)e->chains.size()) return set_err("%s: bad chain %d", who, chain);
+    return 0;
+}
+
+int dqmc_read_green(dqmc_engine *e, int chain, double *G)
+{
+    if (chain_ok(e, chain, "dqmc_read_green")) return 1;
+    const int n = e->hdev[chain].n;
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(G, e->hdev[chain].G, (size_t)n * n * 8, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int dqmc_read_field(dqmc_engine *e, int chain, signed char *field)
+{
+    if (chain_ok(e, chain, "dqmc_read_field")) return 1;
+    const DqmcChainDev &d = e->hdev[chain];
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(field, d.field, (size_t)d.L * d.n, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int dqmc_write_field(dqmc_engine *e, int chain, const signed char *field)
+{
+    if (chain_ok(e, chain, "dqmc_write_field")) return 1;
+    const DqmcChainDev &d = e->hdev[chain];
+    for (size_t k = 0; k < (size_t)d.L * d.n; ++k)
+        if (field[k] != 1 && field[k] != -1) return set_err("field entries must be +/-1");
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(d.field, field, (size_t)d.L * d.n, cudaMemcpyHostToDevice));
+    dq::k_init<<<1, DQMC_NT, e->smem, e->stream>>>(e->dchains + chain, e->dmodels);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(e->stream));
+    return 0;
+}
+
+int dqmc_read_counters(dqmc_engine *e, int chain, dqmc_chain_counters *out)
+{
+    if (chain_ok(e, chain, "dqmc_read_counters")) return 1;
+    DqmcChainDev d;
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(&d, e->dchains + chain, sizeof d, cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof *out);
+    out->attempts = d.attempts;
+    out->accepted = d.accepted;
+    out->sweeps = d.sweeps;
+    out->status = d.status;
+    out->sign = d.sign;
+    out->drift_max = d.drift_max;
+    out->drift_mean = d.drift_count ? d.drift_sum / (double)d.drift_count : 0.0;
+    out->drift_samples = d.drift_count;
+    out->scratch_drift_max = d.sdrift_max;
+    out->scratch_drift_mean = d.sdrift_count ? d.sdrift_sum / (double)d.sdrift_count : 0.0;
+    out->scratch_drift_samples = d.sdrift_count;
+    for (int i = 0; i < 4; ++i) out->rng[i] = d.rng[i];
+    return 0;
+}
+
+int dqmc_read_bins(dqmc_engine *e, int chain, double *scalars, double *szz, double *sperp)
+{
+    if (chain_ok(e, chain, "dqmc_read_bins")) return 1;
+    const DqmcChainDev &d = e->hdev[chain];
+    const HModel &m = e->models[e->chains[chain].model];
+    CU(cudaStreamSynchronize(e->stream));
+    if (scalars)
+        CU(cudaMemcpy(scalars, d.bins, (size_t)e->nbin * DQMC_BIN_FIELDS * 8,
+                      cudaMemcpyDeviceToHost));
+    if (szz && m.nq_zz)
+        CU(cudaMemcpy(szz, d.bins_zz, (size_t)e->nbin * m.nq_zz * 8, cudaMemcpyDeviceToHost));
+    if (sperp && m.nq_perp)
+        CU(cudaMemcpy(sperp, d.bins_perp, (size_t)e->nbin * m.nq_perp * 8,
+                      cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int dqmc_read_profile(dqmc_engine *e, int chain, unsigned long long *cycles, int count)
+{
+    if (chain_ok(e, chain, "dqmc_read_profile")) return 1;
+    DqmcChainDev d;
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(&d, e->dchains + chain, sizeof d, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < count && i < DQMC_PH_COUNT; ++i) cycles[i] = d.prof[i];
+    return 0;
+}
+
+int dqmc_clear_bins(dqmc_engine *e)
+{
+    if (check_prepared(e, "dqmc_clear_bins")) return 1;
+    for (size_t k = 0; k < e->chains.size(); ++k) {
+        const DqmcChainDev &d = e->hdev[k];
+        const HModel &m = e->models[e->chains[k].model];
+        CU(cudaMemsetAsync(d.bins, 0, (size_t)e->nbin * DQMC_BIN_FIELDS * 8, e->stream));
+        if (m.nq_zz) CU(cudaMemsetAsync(d.bins_zz, 0, (size_t)e->nbin * m.nq_zz * 8, e->stream));
+        if (m.nq_perp)
+            CU(cudaMemsetAsync(d.bins_perp, 0, (size_t)e->nbin * m.nq_perp * 8, e->stream));
+    }
+    CU(cudaStreamSynchronize(e->stream));
+    return 0;
+}
+
+int dqmc_green_from_scratch(dqmc_engine *e, int chain, int l0, double *G, int *det_sign)
+{
+    if (chain_ok(e, chain, "dqmc_green_from_scratch")) return 1;
+    const DqmcChainDev &d = e->hdev[chain];
+    if (l0 < 0 || l0 >= d.L) return set_err("l0 out of range");
+    double *dG = nullptr;
+    int *ddet = nullptr;
+    CU(cudaMalloc(&dG, (size_t)d.n * d.n * 8 + 16));
+    ddet = (int *)(dG + (size_t)d.n * d.n);
+    dq::k_scratch<<<1, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels, chain, l0, dG, ddet);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err == cudaSuccess) err = cudaMemcpy(G, dG, (size_t)d.n * d.n * 8, cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess) err = cudaMemcpy(det_sign, ddet, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(dG);
+    if (err != cudaSuccess) return set_err("dqmc_green_from_scratch: %s", cudaGetErrorString(err));
+    return 0;
+}
+
+int dqmc_wrap_green(dqmc_engine *e, int chain, int l, double *G)
+{
+    if (chain_ok(e, chain, "dqmc_wrap_green")) return 1;
+    const DqmcChainDev &d = e->hdev[chain];
+    if (l < 0 || l >= d.L) return set_err("l out of range");
+    double *dG = nullptr;
+    const size_t bytes = (size_t)d.n * d.n * 8;
+    CU(cudaMalloc(&dG, bytes));
+    cudaError_t err = cudaMemcpy(dG, G, bytes, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) {
+        dq::k_wrap<<<1, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels, chain, l, dG);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err == cudaSuccess) err = cudaMemcpy(G, dG, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dG);
+    if (err != cudaSuccess) return set_err("dqmc_wrap_green: %s", cudaGetErrorString(err));
+    return 0;
+}
+
+/* Host sign of det(U) for a small orthogonal U (partial-pivot LU). */
+static int host_det_sign(int n, const double *U)
+{
+    std::vector<double> a(U, U + (size_t)n * n);
+    int s = 1;
+    for (int j = 0; j < n; ++j) {
+        int p = j;
+        for (int i = j + 1; i < n; ++i)
+            if (std::fabs(a[i + (size_t)j * n]) > std::fabs(a[p + (size_t)j * n])) p = i;
+        if (a[p + (size_t)j * n] == 0.0) return 0;
+        if (p != j) {
+            s = -s;
+            for (int c = 0; c < n; ++c) std::swap(a[j + (size_t)c * n], a[p + (size_t)c * n]);
+        }
+        if (a[j + (size_t)j * n] < 0) s = -s;
+        for (int i = j + 1; i < n; ++i) {
+            const double f = a[i + (size_t)j * n] / a[j + (size_t)j * n];
+            for (int c = j + 1; c < n; ++c) a[i + (size_t)c * n] -= f * a[j + (size_t)c * n];
+        }
+    }
+    return s;
+}
+
+int dqmc_udv_green(int device, int n, const double *U, const double *D, const double *T,
+                   double *G, int *det_sign)
+{
+    if (n <= 0 || n > DQMC_MAX_N || !U || !D || !T || !G || !det_sign)
+        return set_err("dqmc_udv_green: bad arguments");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err("dqmc_udv_green: no CUDA device");
+    CU(cudaSetDevice(device));
+    const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
+    /* signed D -> positive D with the signs moved into U's columns */
+    std::vector<double> slot(usz, 0.0);
+    int dsign = host_det_sign(n, U);
+    for (int j = 0; j < n; ++j) {
+        const double sgn = D[j] < 0 ? -1.0 : 1.0;
+        if (D[j] < 0) dsign = -dsign;
+        for (int i = 0; i < n; ++i) slot[i + (size_t)j * n] = U[i + (size_t)j * n] * sgn;
+        slot[2 * nn + j] = std::log(std::fabs(D[j]));
+    }
+    std::memcpy(slot.data() + nn, T, nn * 8);
+    slot[2 * nn + n] = dsign;
+    const size_t twsz = (size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB * DQMC_QNB;
+    char *buf = nullptr;
+    const size_t bytes = usz * 8 + (3 * nn + twsz) * 8 + nn * 8 + 64;
+    CU(cudaMalloc(&buf, bytes));
+    double *dslot = (double *)buf;
+    double *ws = dslot + usz;
+    double *dG = ws + 3 * nn + twsz;
+    int *ddet = (int *)(dG + nn);
+    cudaError_t err = cudaMemcpy(dslot, slot.data(), usz * 8, cudaMemcpyHostToDevice);
+    const size_t sm = dq::smem_doubles(n, 1) * 8;
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(dq::k_udv_green, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sm);
+    if (err == cudaSuccess) {
+        dq::k_udv_green<<<1, DQMC_NT, sm>>>(n, dslot, ws, dG, ddet);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    if (err == cudaSuccess) err = cudaMemcpy(G, dG, nn * 8, cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess) err = cudaMemcpy(det_sign, ddet, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (err != cudaSuccess) return set_err("dqmc_udv_green: %s", cudaGetErrorString(err));
+    return 0;
+}
+
+}  /* extern "C" */

@@ -1,0 +1,485 @@
+/* Sweep, measurement and test kernels.  One CTA = one chain. */
+#pragma once
+#include "dqmc_device.cuh"
+
+namespace dq {
+
+enum { KF_MEASURE = 1, KF_SDRIFT = 2, KF_STAB_DRIFT = 4 };
+
+/* Phase timer: thread 0 charges the cycles since the last mark to a phase.
+ * Phases end at a CTA barrier, so thread 0's clock covers all threads. */
+struct PhaseClock {
+    long long t;
+    __device__ __forceinline__ void mark() { t = clock64(); }
+    __device__ __forceinline__ void charge(DqmcChainDev *ch, int ph)
+    {
+        if (threadIdx.x == 0) {
+            const long long now = clock64();
+            ch->prof[ph] += (unsigned long long)(now - t);
+            t = now;
+        }
+    }
+};
+
+__device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
+{
+    return Scr{ch->w[0], ch->w[1], ch->w[2], ch->twall};
+}
+
+/* One site block of the delayed update (green.c:384-480 restated as a
+ * submatrix update).  With S the block's sites and g = G[S,S] at block
+ * start, every accepted flip keeps G_cur = G - X Gam Y, X = (I - G)[:,S],
+ * Y = G[S,:], with Gam supported on the accepted sites only:
+ *   x = (I + Gam g) e_a,  y^T = e_a^T (I - (I - g) Gam),  Gam += f x y^T,
+ * and the block's own entries gt = G_cur[S,S] follow the rank-1 update of
+ * green_delay_accept.  The ratio uses gt[a,a] exactly as
+ * green_delay_ratio_N / green_ph_down_ratio_N (green.c:402-416).  After the
+ * block, G -= (X Gam)[:,A] Y[A,:] is one rank-m GEMM.  Warp 0 runs the
+ * proposals (one RNG draw per site, always consumed: dqmc.c:666-668). */
+__device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *G, signed char *fl,
+                           const DqmcModelDev &md, uint64_t *rng,
+                           unsigned long long *att, unsigned long long *acc,
+                           double *Zs, double *Ys, Smem &s, DqmcChainDev *ch,
+                           PhaseClock &pc)
+{
+    const int ld = kb + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *g0 = s.g0, *gt = s.gt, *gam = s.gam, *xs = s.xs, *colA = s.colA;
+    int *alist = s.iscr;
+    for (int e = threadIdx.x; e < kbs * kbs; e += NT) {
+        const int r = e % kbs, c = e / kbs;
+        const double v = G[(i0 + r) + (size_t)(i0 + c) * n];
+        g0[r + c * ld] = v;
+        gt[r + c * ld] = v;
+        gam[r + c * ld] = 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int m = 0;
+        for (int a = 0; a < kbs; ++a) {
+            const signed char sv = fl[i0 + a];
+            const int si = sv > 0;
+            const double Nu = md.Nup[si], Nd = md.Ndn[si];
+            const double gii = gt[a + a * ld];
+            const double Ru = 1.0 + (1.0 - gii) * Nu;
+            const double Rd = 1.0 + gii * Nd;
+            const double R = Ru * Rd;
+            double u = 0.0;
+            if (lane == 0) {
+                u = rng_next(rng);
+                ++*att;
+            }
+            u = __shfl_sync(FULL, u, 0);
+            if (u < fabs(R)) {
+                const double fac = Nu / Ru;
+                double yv[2], ra[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int b = lane + 32 * h;
+                    yv[h] = 0.0;
+                    ra[h] = 0.0;
+                    if (b < kbs) {
+                        double x = (b == a) ? 1.0 : 0.0, y = x;
+                        for (int c = 0; c < kbs; ++c) {
+                            x += gam[b + c * ld] * g0[c + a * ld];
+                            y -= ((c == a) ? 1.0 - g0[a + c * ld] : -g0[a + c * ld]) *
+                                 gam[c + b * ld];
+                        }
+                        xs[b] = x;
+                        colA[b] = gt[b + a * ld];
+                        yv[h] = y;
+                        ra[h] = gt[a + b * ld];
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int b = lane + 32 * h;
+                    if (b < kbs) {
+                        const double fy = fac * yv[h], fr = fac * ra[h];
+                        for (int c = 0; c < kbs; ++c) {
+                            gam[c + b * ld] += xs[c] * fy;
+                            gt[c + b * ld] -= ((c == a) ? 1.0 - colA[c] : -colA[c]) * fr;
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    fl[i0 + a] = (signed char)(-sv);
+                    ++*acc;
+                    alist[m] = a;
+                }
+                ++m;
+            }
+        }
+        if (lane == 0) s.iscr[2 * DQMC_MAX_KB] = m;
+    }
+    __syncthreads();
+    pc.charge(ch, DQMC_PH_PROPOSE);
+    const int m = s.iscr[2 * DQMC_MAX_KB];
+    if (m == 0) return;
+    /* Z = X[:,A] Gam[A,A] and Y[A,:] from G before it changes */
+    gemm_sq<true, true>(
+        n, m, m,
+        [=](int i, int k) {
+            const int col = i0 + alist[k];
+            return (i == col ? 1.0 : 0.0) - G[i + (size_t)col * n];
+        },
+        [=](int k, int j) { return gam[alist[k] + alist[j] * ld]; },
+        [=](int i, int j, double v) { Zs[i + (size_t)j * n] = v; }, s.gsm);
+    for (int e = threadIdx.x; e < m * n; e += NT) {
+        const int q = e % m, c = e / m;
+        Ys[q + (size_t)c * kb] = G[(i0 + alist[q]) + (size_t)c * n];
+    }
+    gemm_sq<true, true>(
+        n, n, m, [=](int i, int k) { return Zs[i + (size_t)k * n]; },
+        [=](int k, int j) { return Ys[k + (size_t)j * kb]; },
+        [=](int i, int j, double v) { G[i + (size_t)j * n] -= v; }, s.gsm);
+    pc.charge(ch, DQMC_PH_FLUSH);
+}
+
+/* max|G - Gn| and G <- Gn */
+__device__ double adopt_green(int n, double *G, const double *Gn, Smem &s)
+{
+    double mx = 0.0;
+    for (int e = threadIdx.x; e < n * n; e += NT) {
+        const double d = fabs(G[e] - Gn[e]);
+        mx = (d > mx || d != d) ? d : mx;
+        G[e] = Gn[e];
+    }
+    return block_reduce<true>(mx, s.red);
+}
+
+__device__ double max_diff(int n, const double *A, const double *B, Smem &s)
+{
+    double mx = 0.0;
+    for (int e = threadIdx.x; e < n * n; e += NT) mx = fmax(mx, fabs(A[e] - B[e]));
+    return block_reduce<true>(mx, s.red);
+}
+
+/* G(l0) from scratch: L single-slice lmuls then (1+UDT)^{-1} (green.c:262).
+ * Uses the chain's scr UDV slot; returns det sign (0 on failure). */
+__device__ __noinline__ int green_scratch(DqmcChainDev *ch, const DqmcModelDev &md, int l0, double *Gout,
+                             double *slot, Smem &s, int *flag)
+{
+    const int n = ch->n, L = ch->L;
+    Udv u = udv_at(slot, n);
+    udv_identity(u, n);
+    for (int k = 0; k < L; ++k) {
+        const int l = (l0 + k) % L;
+        udv_lmul(n, u, nullptr, md.expK, ch->field + (size_t)l * n, md.expv[0], md.expv[1],
+                 chain_scr(ch), s, flag);
+        if (*flag) return 0;
+    }
+    const int ds = udv_green(n, u, Gout, chain_scr(ch), s, flag);
+    return *flag ? 0 : ds;
+}
+
+/* The forward sweep, dqmc_sweep_forward (dqmc.c:609-813) with
+ * carry_prefix = 0, use_ph = 1 and the combine rebuild.  Returns false on a
+ * numerical failure (flag holds the reason). */
+__device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md, int kflags, Smem &s,
+                           int *flag, uint64_t *rng, unsigned long long *att,
+                           unsigned long long *acc, double *slot_scr)
+{
+    const int n = ch->n, L = ch->L, stab = ch->stab, M = ch->M, kb = ch->kb;
+    const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
+    const Scr w = chain_scr(ch);
+    double *G = ch->G, *Gn = ch->w[3], *tmp = ch->w[4], *tmp2 = ch->w[5];
+    const double v0 = md.expv[0], v1 = md.expv[1];
+    auto Sj = [&](int j) { return udv_at(ch->S + (size_t)j * usz, n); };
+    Udv left = udv_at(ch->left, n), comb = udv_at(ch->comb, n);
+    PhaseClock pc;
+    pc.mark();
+
+    /* Block products B(b_{j+1}, b_j) of the current field.  After the first
+     * sweep they are the ones the previous sweep's left pass computed. */
+    if (!ch->bvalid) {
+        for (int j = 1; j < M; ++j) {
+            const int b0 = j * stab, b1 = min((j + 1) * stab, L);
+            bblock(n, b0, b1 - b0, ch->field, md.expK, v0, v1, ch->bcache + j * nn, tmp, tmp2,
+                   s);
+        }
+    }
+    pc.charge(ch, DQMC_PH_BCACHE);
+    /* suffix stack (green_stack_build_suffix, green.c:203-226) */
+    udv_identity(Sj(M), n);
+    for (int j = M - 1; j >= 1; --j) {
+        udv_copy(Sj(j), Sj(j + 1), n);
+        udv_rmul(n, Sj(j), ch->bcache + j * nn, w, s, flag);
+        if (*flag) return false;
+    }
+    udv_identity(left, n);
+    pc.charge(ch, DQMC_PH_STACK);
+    int tau_left = 0;
+    for (int l = 0; l < L; ++l) {
+        signed char *fl = ch->field + (size_t)l * n;
+        for (int i0 = 0; i0 < n; i0 += kb)
+            site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs, ch->Ys,
+                       s, ch, pc);
+        wrap_green(n, G, tmp, md.expK, md.expKinv, fl, v0, v1, md.expvinv[0], md.expvinv[1],
+                   s);
+        pc.charge(ch, DQMC_PH_WRAP);
+        const bool boundary = ((l + 1) % stab == 0) && (l + 1 < L);
+        const bool last = (l + 1 == L);
+        if (!boundary && !last) continue;
+        const int tau = boundary ? l + 1 : 0;
+        if (kflags & KF_SDRIFT) {
+            const int ds = green_scratch(ch, md, tau, Gn, slot_scr, s, flag);
+            if (*flag || ds == 0) return false;
+            const double d = max_diff(n, G, Gn, s);
+            if (threadIdx.x == 0) {
+                ch->sdrift_count++;
+                ch->sdrift_sum += d;
+                if (d > ch->sdrift_max || ch->sdrift_count == 1) ch->sdrift_max = d;
+            }
+            pc.charge(ch, DQMC_PH_SDRIFT);
+        }
+        const int te = boundary ? l + 1 : L;
+        const int jblk = (boundary ? (l + 1) / stab : M) - 1;
+        if (te > tau_left) {
+            bblock(n, tau_left, te - tau_left, ch->field, md.expK, v0, v1,
+                   ch->bcache + jblk * nn, tmp, tmp2, s);
+            pc.charge(ch, DQMC_PH_BBLOCK);
+            udv_lmul(n, left, ch->bcache + jblk * nn, nullptr, nullptr, 0.0, 0.0, w, s, flag);
+            if (*flag) return false;
+            pc.charge(ch, DQMC_PH_LMUL);
+        }
+        tau_left = te;
+        int ds;
+        if (boundary) {
+            udv_combine(n, left, Sj((l + 1) / stab), comb, w, s, flag);
+            if (*flag) return false;
+            pc.charge(ch, DQMC_PH_COMBINE);
+            ds = udv_green(n, comb, Gn, w, s, flag);
+        } else {
+            ds = udv_green(n, left, Gn, w, s, flag);
+        }
+        pc.charge(ch, DQMC_PH_GREEN);
+        if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
+        __syncthreads();
+        if (*flag) return false;
+        const double d = adopt_green(n, G, Gn, s);
+        if (threadIdx.x == 0) {
+            ch->drift_count++;
+            ch->drift_sum += d;
+            if (d > ch->drift_max || ch->drift_count == 1) ch->drift_max = d;
+            ch->sign = 1.0;
+        }
+        pc.charge(ch, DQMC_PH_ADOPT);
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(NT, 1)
+    k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps)
+{
+    extern __shared__ double smraw[];
+    __shared__ int flag;
+    __shared__ uint64_t rng[4];
+    __shared__ unsigned long long att, acc;
+    DqmcChainDev *ch = &chains[blockIdx.x];
+    const DqmcModelDev &md = models[ch->model];
+    if (threadIdx.x == 0) flag = ch->status;
+    __syncthreads();
+    if (flag) return;
+    Smem s = carve(smraw, ch->n, ch->kb);
+    for (int sw = 0; sw < nsweeps; ++sw) {
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < 4; ++i) rng[i] = ch->rng[i];
+            att = 0;
+            acc = 0;
+            ch->meas_accepted = ch->accepted;
+            ch->meas_attempts = ch->attempts;
+        }
+        __syncthreads();
+        const bool ok = sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < 4; ++i) ch->rng[i] = rng[i];
+            ch->attempts += att;
+            ch->accepted += acc;
+            if (ok && !flag) {
+                ch->sweeps++;
+                ch->bvalid = 1;
+            } else {
+                ch->status = flag ? flag : DQMC_ST_NONFINITE;
+                ch->sign = 0.0;
+                ch->bvalid = 0;
+            }
+        }
+        __syncthreads();
+        if (!ok || flag) return;
+    }
+}
+
+/* G from scratch at l0 = 0 for every chain (dqmc_init_modes, dqmc.c:466-483). */
+__global__ void __launch_bounds__(NT, 1) k_init(DqmcChainDev *chains, const DqmcModelDev *models)
+{
+    extern __shared__ double smraw[];
+    __shared__ int flag;
+    DqmcChainDev *ch = &chains[blockIdx.x];
+    const DqmcModelDev &md = models[ch->model];
+    if (threadIdx.x == 0) flag = 0;
+    __syncthreads();
+    Smem s = carve(smraw, ch->n, ch->kb);
+    const int ds = green_scratch(ch, md, 0, ch->G, ch->scr, s, &flag);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ch->status = flag ? flag : (ds == 0 ? DQMC_ST_DETSIGN : 0);
+        ch->sign = ch->status ? 0.0 : 1.0;
+        ch->bvalid = 0;
+    }
+}
+
+/* Test kernels: rebuild from scratch into out; wrap a caller G. */
+__global__ void __launch_bounds__(NT, 1)
+    k_scratch(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l0, double *out,
+              int *det)
+{
+    extern __shared__ double smraw[];
+    __shared__ int flag;
+    DqmcChainDev *ch = &chains[c];
+    const DqmcModelDev &md = models[ch->model];
+    if (threadIdx.x == 0) flag = 0;
+    __syncthreads();
+    Smem s = carve(smraw, ch->n, ch->kb);
+    const int ds = green_scratch(ch, md, l0, out, ch->scr, s, &flag);
+    if (threadIdx.x == 0) *det = flag ? 0 : ds;
+}
+
+__global__ void __launch_bounds__(NT, 1)
+    k_wrap(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l, double *Gio)
+{
+    extern __shared__ double smraw[];
+    DqmcChainDev *ch = &chains[c];
+    const DqmcModelDev &md = models[ch->model];
+    Smem s = carve(smraw, ch->n, ch->kb);
+    const int n = ch->n;
+    wrap_green(n, Gio, ch->w[4], md.expK, md.expKinv, ch->field + (size_t)l * n, md.expv[0],
+               md.expv[1], md.expvinv[0], md.expvinv[1], s);
+}
+
+/* Caller UDV -> G (fixture parity).  ws: 4 n*n scratch + tw + UDV slot. */
+__global__ void __launch_bounds__(NT, 1)
+    k_udv_green(int n, double *slot, double *ws, double *G, int *det)
+{
+    extern __shared__ double smraw[];
+    __shared__ int flag;
+    if (threadIdx.x == 0) flag = 0;
+    __syncthreads();
+    Smem s = carve(smraw, n, 1);
+    const size_t nn = (size_t)n * n;
+    Scr w{ws, ws + nn, ws + 2 * nn, ws + 3 * nn};
+    const int ds = udv_green(n, udv_at(slot, n), G, w, s, &flag);
+    if (threadIdx.x == 0) *det = flag ? 0 : ds;
+}
+
+/* Equal-time measurements on G_up at slice 0, fused: one read of G gives
+ * measure_sample (measure.c:6-39) with G_down = I - P G_up^T P, the spin
+ * correlations by displacement (structure_factor.c:258-297, 328-392) and the
+ * cosine transforms (finish_fourier, structure_factor.c:311-326); the
+ * sample is added to bin `bin` (replica_bin_add, replica.c:48-71;
+ * q_add, replica.c:219-226).  Per displacement the i order matches the
+ * reference's loop, so the sums are formed in the same order. */
+__global__ void __launch_bounds__(NT)
+    k_measure(DqmcChainDev *chains, const DqmcModelDev *models, int bin)
+{
+    extern __shared__ double smraw[];
+    __shared__ double red[40];
+    DqmcChainDev *ch = &chains[blockIdx.x];
+    if (ch->status) return;
+    PhaseClock pc;
+    pc.mark();
+    const DqmcModelDev &md = models[ch->model];
+    const int n = ch->n;
+    const double *G = ch->G;
+    const double *t = md.thop;
+    const int *p = md.bipart;
+    double ek = 0.0, ei = 0.0, nt = 0.0, bad = 0.0;
+    for (int e = threadIdx.x; e < n * n; e += NT) {
+        const int i = e % n, j = e / n;
+        const double dij = (i == j) ? 1.0 : 0.0;
+        const double gu_ji = G[j + (size_t)i * n];
+        const double gd_ji = dij - (double)(p[j] * p[i]) * G[i + (size_t)j * n];
+        const double tij = t[i + (size_t)j * n];
+        ek += tij * (dij - gu_ji);
+        ek += tij * (dij - gd_ji);
+        bad += isfinite(gu_ji) ? 0.0 : 1.0;
+    }
+    for (int i = threadIdx.x; i < n; i += NT) {
+        const double gu = G[i + (size_t)i * n];
+        const double gd = 1.0 - (double)(p[i] * p[i]) * gu;
+        const double nu = 1.0 - gu, nd = 1.0 - gd;
+        ei += nu * nd;
+        nt += nu + nd;
+    }
+    ek = block_reduce<false>(ek, red);
+    ei = block_reduce<false>(ei, red);
+    nt = block_reduce<false>(nt, red);
+    bad = block_reduce<false>(bad, red);
+    if (bad != 0.0) {
+        if (threadIdx.x == 0) ch->status |= DQMC_ST_NONFINITE;
+        return;
+    }
+    double *cz = smraw, *cp = smraw + n;
+    const int Lx = md.Lx > 0 ? md.Lx : n, Ly = md.Ly > 0 ? md.Ly : 1;
+    const bool spin = (md.nq_zz > 0 || md.nq_perp > 0);
+    if (spin) {
+        for (int d = threadIdx.x; d < n; d += NT) {
+            const int dx = d % Lx, dy = d / Lx;
+            double sz = 0.0, sp = 0.0;
+            for (int i = 0; i < n; ++i) {
+                const int xi = i % Lx, yi = i / Lx;
+                const int xj = (xi - dx + Lx) % Lx, yj = (yi - dy + Ly) % Ly;
+                const int j = xj + yj * Lx;
+                const double delta = (i == j) ? 1.0 : 0.0;
+                const double pij = (double)(p[i] * p[j]);
+                const double gu_ii = G[i + (size_t)i * n], gu_jj = G[j + (size_t)j * n];
+                const double gu_ij = G[i + (size_t)j * n], gu_ji = G[j + (size_t)i * n];
+                const double gd_ii = 1.0 - (double)(p[i] * p[i]) * gu_ii;
+                const double gd_jj = 1.0 - (double)(p[j] * p[j]) * gu_jj;
+                const double gd_ij = delta - pij * gu_ji;
+                const double gd_ji = delta - pij * gu_ij;
+                const double spin_i = gd_ii - gu_ii, spin_j = gd_jj - gu_jj;
+                sz += 0.25 * (spin_i * spin_j + (delta - gu_ji) * gu_ij + (delta - gd_ji) * gd_ij);
+                sp += 0.5 * ((delta - gu_ji) * gd_ij + (delta - gd_ji) * gu_ij);
+            }
+            cz[d] = sz;
+            cp[d] = sp;
+        }
+        __syncthreads();
+    }
+    double *bins = ch->bins + (size_t)bin * DQMC_BIN_FIELDS;
+    if (threadIdx.x == 0) {
+        const double U = md.U, mu = md.mu, sign = ch->sign;
+        const double ekin = ek, eint = U * ei, ntot = nt, dbl = ei / n;
+        const double E = ekin + eint;
+        bins[DQMC_BIN_EHUB] += sign * E;
+        bins[DQMC_BIN_EGC] += sign * (E - mu * ntot);
+        bins[DQMC_BIN_EPH] += sign * (E - 0.5 * U * ntot + 0.25 * U * (double)n);
+        bins[DQMC_BIN_N] += sign * ntot;
+        bins[DQMC_BIN_D] += sign * dbl;
+        bins[DQMC_BIN_SIGN] += sign;
+        bins[DQMC_BIN_COUNT] += 1.0;
+        bins[DQMC_BIN_ACCEPTED] += (double)(ch->accepted - ch->meas_accepted);
+        bins[DQMC_BIN_ATTEMPTS] += (double)(ch->attempts - ch->meas_attempts);
+    }
+    if (spin) {
+        const double sign = ch->sign;
+        for (int q = threadIdx.x; q < md.nq_zz; q += NT) {
+            double sum = 0.0;
+            for (int d = 0; d < n; ++d) sum += md.cos_zz[d + (size_t)q * n] * cz[d];
+            ch->bins_zz[(size_t)bin * md.nq_zz + q] += sign * (sum / (double)n);
+        }
+        for (int q = threadIdx.x; q < md.nq_perp; q += NT) {
+            double sum = 0.0;
+            for (int d = 0; d < n; ++d) sum += md.cos_perp[d + (size_t)q * n] * cp[d];
+            ch->bins_perp[(size_t)bin * md.nq_perp + q] += sign * (sum / (double)n);
+        }
+    }
+    __syncthreads();
+    pc.charge(ch, DQMC_PH_MEASURE);
+}
+
+}  // namespace dq

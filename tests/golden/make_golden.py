@@ -1,0 +1,119 @@
+"""Generate the golden parity fixtures from the UNMODIFIED reference.
+
+Run in a container where the reference sources exist (``$SAIQMC_REF``,
+default /root/reference): ``python tests/golden/make_golden.py``.  It
+builds oracle/_ref (oracle/build.py), drives the reference engine through
+oracle/ref_shim.c and writes small .npz files next to this script.  The
+reference's own UDV fixtures (tests/fixtures/udv_phase6a_*.txt, read here as
+data) are re-packed into udv_fixture.npz.  The GPU box never needs the
+reference: tests read only the .npz files.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import build as obuild  # noqa: E402
+from oracle.bind import LAT_CHAIN, LAT_SQUARE, Reference  # noqa: E402
+
+REF = os.environ.get("SAIQMC_REF", "/root/reference")
+
+# (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, selector)
+CASES = [
+    ("chain4_b2", LAT_CHAIN, 4, 1, 4.0, 0.1, 20, 8, 1, 4, "all"),
+    ("chain4_u0", LAT_CHAIN, 4, 1, 0.0, 0.1, 20, 8, 5, 2, "all"),
+    ("sq4_b4", LAT_SQUARE, 4, 4, 4.0, 0.1, 40, 10, 7, 3, "all"),
+    ("sq6_b2", LAT_SQUARE, 6, 6, 6.0, 0.1, 20, 8, 3, 3, "af"),
+    ("sq8_b4", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 2, "af"),
+]
+
+
+def _read_tokens(path):
+    with open(path) as f:
+        return f.read().split()
+
+
+def udv_fixture(out):
+    d = os.path.join(REF, "tests", "fixtures")
+    tok = _read_tokens(os.path.join(d, "udv_phase6a_actual_n16.txt"))
+    it = iter(tok)
+    rec = {}
+    key = None
+    vals = []
+    for t in it:
+        try:
+            vals.append(float(t))
+        except ValueError:
+            if key is not None:
+                rec[key] = vals
+            key, vals = t, []
+    rec[key] = vals
+    n = int(rec["n"][0])
+    U = np.array(rec["U"]).reshape(n, n).T       # file is column-major
+    D = np.array(rec["D"])
+    T = np.array(rec["T"]).reshape(n, n).T
+    gtok = _read_tokens(os.path.join(d, "udv_phase6a_actual_n16_green.txt"))
+    ds = int(gtok[gtok.index("det_sign") + 1])
+    g0 = gtok.index("G") + 1
+    G = np.array([float(x) for x in gtok[g0:g0 + n * n]]).reshape(n, n).T
+    np.savez_compressed(out, U=U, D=D, T=T, G=G, det_sign=ds,
+                        offset=float(rec["offset"][0]),
+                        min_logD=float(rec["min_logD"][0]),
+                        max_logD=float(rec["max_logD"][0]))
+
+
+def main():
+    obuild.build_ref()
+    R = Reference()
+    # RNG streams and replica seeds (rng.c:17-37, replica.c:17-34)
+    seeds = np.array([1, 7, 11, 12345, 2**63 + 5], dtype=np.uint64)
+    draws = np.stack([R.rng(int(s), 16) for s in seeds])
+    rs = [(12345, 0, 0), (12345, 3, 0), (12345, 0, 1), (12345, 2, 7), (1, 5, 3)]
+    rseed = np.array([R.replica_seed(*t) for t in rs], dtype=np.uint64)
+    jk_x = np.array([1.0, 3.0, 5.0, 2.5, -1.0])
+    jk = np.array(R.jackknife(jk_x))
+    np.savez_compressed(os.path.join(HERE, "rng.npz"), seeds=seeds, draws=draws,
+                        replica_args=np.array(rs, dtype=np.int64), replica_seeds=rseed,
+                        jk_x=jk_x, jk=jk)
+    for (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, sel) in CASES:
+        ch = R.chain(kind, Lx, Ly, U, dtau, L, stab, seed, drift=True)
+        model = R.model(ch)
+        st0 = ch.state()
+        rc, gs, ds = ch.green_scratch(0)
+        # one wrap of the initial G at slice 0
+        gw = ch.wrap(0, st0["Gu"])
+        fields, Gs, cnt, meas, szz, sperp = [], [], [], [], [], []
+        for _ in range(sweeps):
+            ch.sweep(1)
+            st = ch.state()
+            fields.append(st["field"])
+            Gs.append(st["Gu"])
+            cnt.append([st["attempts"], st["accepted"], st["sweeps"], st["status"]])
+            m, z, p = R.measure(ch, sel)
+            meas.append(m)
+            szz.append(z)
+            sperp.append(p)
+        np.savez_compressed(
+            os.path.join(HERE, f"{name}.npz"),
+            params=np.array([kind, Lx, Ly, L, stab, seed, sweeps], dtype=np.int64),
+            U=U, dtau=dtau, selector=sel,
+            expK=model["expK"], expKinv=model["expKinv"], thop=model["thop"],
+            bipart=model["bipart"], field0=st0["field"], G0=st0["Gu"],
+            G_scratch=gs, det_sign=ds, G_wrap0=gw,
+            fields=np.array(fields), Gs=np.array(Gs),
+            counters=np.array(cnt, dtype=np.int64), meas=np.array(meas),
+            szz=np.array(szz), sperp=np.array(sperp), drift=R.drift(ch),
+            rng_end=st["rng"])
+        ch.free()
+    udv_fixture(os.path.join(HERE, "udv_fixture.npz"))
+    print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
+
+
+if __name__ == "__main__":
+    main()
