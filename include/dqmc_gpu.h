@@ -52,7 +52,9 @@ typedef struct {
                         at every stabilization (on by default); SCRATCH =
                         also the reference's rebuild-from-scratch drift
                         (src/dqmc.c:64-98, costly)                            */
-    int reserved[8];
+    int ctas_per_sm; /* sweep kernel residency: 0 = auto (two chains per SM
+                        when there are more chains than SMs), 1 or 2      */
+    int reserved[7];
 } dqmc_engine_desc;
 
 typedef struct {
@@ -66,6 +68,9 @@ typedef struct {
     unsigned long long drift_samples;
     double scratch_drift_max, scratch_drift_mean;  /* reference drift */
     unsigned long long scratch_drift_samples;
+    int scratch_drift_max_tau;     /* tau and sweep of the maximum   */
+    int pad2;
+    unsigned long long scratch_drift_max_sweep;
     uint64_t rng[4];               /* xoshiro256** state (src/rng.h:6-8) */
 } dqmc_chain_counters;
 

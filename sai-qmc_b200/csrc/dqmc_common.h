@@ -10,7 +10,7 @@
 
 #define DQMC_NT 256          /* threads per CTA; one CTA owns one chain   */
 #define DQMC_MAX_N 1024      /* largest lattice the kernels are laid out for */
-#define DQMC_MAX_KB 64       /* largest site block of the delayed update    */
+#define DQMC_MAX_KB 32       /* largest site block of the delayed update (one lane per column) */
 #define DQMC_QNB 16          /* Householder panel width                     */
 
 /* status bits (per chain, sticky; a chain with status != 0 is frozen)     */
@@ -75,7 +75,8 @@ typedef struct {
     unsigned long long drift_count;
     /* reference-style drift (rebuild from scratch), opt-in                 */
     double sdrift_max, sdrift_sum;
-    unsigned long long sdrift_count;
+    unsigned long long sdrift_count, sdrift_max_sweep;
+    int sdrift_max_tau;
     /* arena pointers */
     signed char *field;        /* L x n */
     double *G;                 /* n x n */

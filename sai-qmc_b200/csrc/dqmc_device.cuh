@@ -11,12 +11,25 @@
 
 #include "dqmc_common.h"
 
-namespace dq {
+/* The device code is compiled twice (dqmc_k1.cu, dqmc_k2.cu) into distinct
+ * namespaces: one CTA per SM with the full register file, and two CTAs per
+ * SM (128 registers, narrower reflector chunks) for large batches. */
+#ifndef DQMC_NS
+#define DQMC_NS dq
+#endif
+#ifndef DQMC_MINB
+#define DQMC_MINB 1
+#endif
+#ifndef DQMC_WCOLS
+#define DQMC_WCOLS 256
+#endif
+
+namespace DQMC_NS {
 
 constexpr int NT = DQMC_NT;
 constexpr int NW = NT / 32;
 constexpr int QNB = DQMC_QNB;
-constexpr int WCOLS = 256;   /* column chunk of a block-reflector update */
+constexpr int WCOLS = DQMC_WCOLS;  /* column chunk of a block-reflector update */
 constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -55,12 +68,20 @@ __device__ double block_reduce(double v, double *red)
 /* Tile configuration: BM x BN output tile, BK-deep k slices, each thread
  * owns a TM x TN register tile at rows ty + TY*r, cols tx + TX*c (strided so
  * that shared-memory reads are broadcast or conflict-free). */
-template <int BM_, int BN_, int BK_, int TM_, int TN_>
+template <int BM_, int BN_, int BK_, int TM_, int TN_, bool MMA_ = false, int WM_ = 2>
 struct Tile {
     static constexpr int BM = BM_, BN = BN_, BK = BK_, TM = TM_, TN = TN_;
+    static constexpr bool MMA = MMA_;
+    /* DMMA layout: WM x WN warps, each FM x FN m16n8 fragments */
+    static constexpr int WM = WM_, WN = NW / WM_;
+    static constexpr int FM = BM / (WM * 16), FN = BN / (WN * 8);
+    static_assert(!MMA || (FM * WM * 16 == BM && FN * WN * 8 == BN && TM == FM * FN && TN == 4),
+                  "DMMA tile shape");
     static constexpr int TX = BN / TN, TY = BM / TM;
-    static_assert(TX * TY == NT, "thread grid must cover the CTA");
-    static constexpr int AP = BM + 1, BP = BN + 1;
+    static_assert(MMA || TX * TY == NT, "thread grid must cover the CTA");
+    /* SIMT tiles pad by one (broadcast/conflict-free reads); DMMA tiles pad
+     * rows to 8 mod 32 banks so a fragment load is two wavefronts. */
+    static constexpr int AP = MMA ? BM + 4 : BM + 1, BP = MMA ? BN + 4 : BN + 1;
     static constexpr int AL = BM * BK / NT, BL = BK * BN / NT;
     static_assert(AL * NT == BM * BK && BL * NT == BK * BN, "load split");
     static constexpr int SMEM = 2 * BK * AP + 2 * BK * BP;
@@ -69,15 +90,37 @@ struct Tile {
 using TSq = Tile<64, 64, 16, 4, 4>;     /* square-ish products            */
 using TSm = Tile<32, 32, 16, 2, 2>;     /* small lattices                 */
 using TWide = Tile<16, 128, 16, 1, 8>;  /* 16-row results (V^T X, trsm)    */
-constexpr int GEMM_SMEM = (TWide::SMEM > TSq::SMEM ? TWide::SMEM : TSq::SMEM);
+/* FP64 tensor-core tiles: 64 x 64 with 8 warps as 2 (M) x 4 (N), warp tile
+ * 32 x 16 = 2 x 2 mma.m16n8k4 fragments; 16 x 128 with 1 x 8 warps. */
+using TMma = Tile<64, 64, 16, 4, 4, true, 2>;
+using TMmaWide = Tile<16, 128, 16, 2, 4, true, 1>;
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int GEMM_SMEM =
+    cmax(cmax(TWide::SMEM, TSq::SMEM), cmax(TMma::SMEM, TMmaWide::SMEM));
+
+/* D = A(16x4) B(4x8) + C, FP64 on the tensor cores (sm_90+ shape). */
+__device__ __forceinline__ void dmma_16x8x4(double *c, double a0, double a1, double b0)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+        "{%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
 
 /* C(M x N) <- epilogue of sum_k la(i,k) * lb(k,j).
  * la/lb are element loaders (any transpose, scaling or gather lives there);
  * AMF: consecutive i are contiguous for la; BKF: consecutive k contiguous
  * for lb -- only affects which thread fetches which element (coalescing).
- * st(i, j, acc) is the epilogue.  Every thread of the CTA must call this. */
-template <class T, bool AMF, bool BKF, class LA, class LB, class ST>
-__device__ void gemm(int M, int N, int K, LA la, LB lb, ST st, double *sm)
+ * Epilogue: st(i, j, acc), or for RMW = true st(i, j, acc, c) with
+ * c = lc(i, j) fetched one output tile ahead (read-modify-write products
+ * such as G -= Z Y overlap the C reads with the previous tile's math).
+ * The (tile, k-slice) sequence is one flat software pipeline: the next
+ * slice -- possibly of the next output tile -- is fetched into registers
+ * while the current one is multiplied, so short-K products stay busy.
+ * Every thread of the CTA must call this. */
+template <class T, bool AMF, bool BKF, bool RMW, class LA, class LB, class LC, class ST>
+__device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, double *sm)
 {
     constexpr int BM = T::BM, BN = T::BN, BK = T::BK, TM = T::TM, TN = T::TN;
     constexpr int TX = T::TX, TY = T::TY, AP = T::AP, BP = T::BP;
@@ -85,57 +128,120 @@ __device__ void gemm(int M, int N, int K, LA la, LB lb, ST st, double *sm)
     double *As = sm;
     double *Bs = sm + 2 * BK * AP;
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+    const int lane = tid & 31, warp = tid >> 5, gid = lane >> 2, tig = lane & 3;
+    const int wm = warp % T::WM, wn = warp / T::WM;
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
     const int nk = (K + BK - 1) / BK;
+    const int total = tm * tn * nk;
+    (void)tn;
+    /* output coordinates of accumulator (r, c) of this thread in a tile */
+    auto out_ij = [&](int r, int c, int &i, int &j) {
+        if constexpr (T::MMA) {
+            const int mi = r / T::FN, ni = r % T::FN;
+            i = wm * (T::FM * 16) + mi * 16 + gid + (c >> 1) * 8;
+            j = wn * (T::FN * 8) + ni * 8 + 2 * tig + (c & 1);
+        } else {
+            i = ty + TY * r;
+            j = tx + TX * c;
+        }
+    };
     __syncthreads();
-    for (int t = 0; t < tm * tn; ++t) {
-        const int m0 = (t % tm) * BM, n0 = (t / tm) * BN;
-        double acc[TM][TN];
+    if (total == 0) return;
+    double ra[AL], rb[BL];
+    /* fetch position (tile origin and k offset), advanced incrementally */
+    int fm0 = 0, fn0 = 0, fk0 = 0;
+    auto advance = [&](int &m0, int &n0, int &k0) {
+        k0 += BK;
+        if (k0 >= nk * BK) {
+            k0 = 0;
+            m0 += BM;
+            if (m0 >= tm * BM) {
+                m0 = 0;
+                n0 += BN;
+            }
+        }
+    };
+    auto fetch = [&]() {
+        const int m0 = fm0, n0 = fn0, k0 = fk0;
+#pragma unroll
+        for (int q = 0; q < AL; ++q) {
+            const int e = tid + q * NT;
+            const int i = AMF ? e % BM : e / BK, k = AMF ? e / BM : e % BK;
+            const int gi = m0 + i, gk = k0 + k;
+            ra[q] = (gi < M && gk < K) ? la(gi, gk) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < BL; ++q) {
+            const int e = tid + q * NT;
+            const int k = BKF ? e % BK : e / BN, j = BKF ? e / BK : e % BN;
+            const int gk = k0 + k, gj = n0 + j;
+            rb[q] = (gk < K && gj < N) ? lb(gk, gj) : 0.0;
+        }
+    };
+    auto put = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < AL; ++q) {
+            const int e = tid + q * NT;
+            const int i = AMF ? e % BM : e / BK, k = AMF ? e / BM : e % BK;
+            As[buf * BK * AP + k * AP + i] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < BL; ++q) {
+            const int e = tid + q * NT;
+            const int k = BKF ? e % BK : e / BN, j = BKF ? e / BK : e % BN;
+            Bs[buf * BK * BP + k * BP + j] = rb[q];
+        }
+    };
+    double cpre[TM][TN];
+    auto fetch_c = [&](int m0, int n0) {
 #pragma unroll
         for (int r = 0; r < TM; ++r)
 #pragma unroll
-            for (int c = 0; c < TN; ++c) acc[r][c] = 0.0;
-        double ra[AL], rb[BL];
-        auto fetch = [&](int k0) {
-#pragma unroll
-            for (int q = 0; q < AL; ++q) {
-                const int e = tid + q * NT;
-                const int i = AMF ? e % BM : e / BK, k = AMF ? e / BM : e % BK;
-                const int gi = m0 + i, gk = k0 + k;
-                ra[q] = (gi < M && gk < K) ? la(gi, gk) : 0.0;
+            for (int c = 0; c < TN; ++c) {
+                int i, j;
+                out_ij(r, c, i, j);
+                i += m0;
+                j += n0;
+                cpre[r][c] = (i < M && j < N) ? lc(i, j) : 0.0;
             }
+    };
+    double acc[TM][TN];
 #pragma unroll
-            for (int q = 0; q < BL; ++q) {
-                const int e = tid + q * NT;
-                const int k = BKF ? e % BK : e / BN, j = BKF ? e / BK : e % BN;
-                const int gk = k0 + k, gj = n0 + j;
-                rb[q] = (gk < K && gj < N) ? lb(gk, gj) : 0.0;
-            }
-        };
-        auto put = [&](int buf) {
+    for (int r = 0; r < TM; ++r)
 #pragma unroll
-            for (int q = 0; q < AL; ++q) {
-                const int e = tid + q * NT;
-                const int i = AMF ? e % BM : e / BK, k = AMF ? e / BM : e % BK;
-                As[buf * BK * AP + k * AP + i] = ra[q];
-            }
+        for (int c = 0; c < TN; ++c) acc[r][c] = 0.0;
+    if constexpr (RMW) fetch_c(0, 0);
+    fetch();
+    put(0);
+    __syncthreads();
+    int cm0 = 0, cn0 = 0, ck0 = 0;   /* position being multiplied */
+    advance(fm0, fn0, fk0);
+    for (int it = 0; it < total; ++it) {
+        const int cur = it & 1;
+        if (it + 1 < total) fetch();
+        const double *a = As + cur * BK * AP;
+        const double *b = Bs + cur * BK * BP;
+        if constexpr (T::MMA) {
+            constexpr int FM = T::FM, FN = T::FN;
 #pragma unroll
-            for (int q = 0; q < BL; ++q) {
-                const int e = tid + q * NT;
-                const int k = BKF ? e % BK : e / BN, j = BKF ? e / BK : e % BN;
-                Bs[buf * BK * BP + k * BP + j] = rb[q];
+            for (int kk = 0; kk < BK; kk += 4) {
+                double a0[FM], a1[FM], b0[FN];
+#pragma unroll
+                for (int mi = 0; mi < FM; ++mi) {
+                    const int i = wm * (FM * 16) + mi * 16 + gid;
+                    a0[mi] = a[(kk + tig) * AP + i];
+                    a1[mi] = a[(kk + tig) * AP + i + 8];
+                }
+#pragma unroll
+                for (int ni = 0; ni < FN; ++ni)
+                    b0[ni] = b[(kk + tig) * BP + wn * (FN * 8) + ni * 8 + gid];
+#pragma unroll
+                for (int mi = 0; mi < FM; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < FN; ++ni)
+                        dmma_16x8x4(acc[mi * FN + ni], a0[mi], a1[mi], b0[ni]);
             }
-        };
-        if (nk > 0) {
-            fetch(0);
-            put(0);
-        }
-        __syncthreads();
-        for (int kt = 0; kt < nk; ++kt) {
-            const int cur = kt & 1;
-            if (kt + 1 < nk) fetch((kt + 1) * BK);
-            const double *a = As + cur * BK * AP;
-            const double *b = Bs + cur * BK * BP;
+        } else {
 #pragma unroll
             for (int k = 0; k < BK; ++k) {
                 double av[TM], bv[TN];
@@ -148,18 +254,54 @@ __device__ void gemm(int M, int N, int K, LA la, LB lb, ST st, double *sm)
 #pragma unroll
                     for (int c = 0; c < TN; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
             }
-            if (kt + 1 < nk) put(cur ^ 1);
-            __syncthreads();
         }
+        if (ck0 == (nk - 1) * BK) {
+            const int m0 = cm0, n0 = cn0;
+            double cv[TM][TN];
+            if constexpr (RMW) {
 #pragma unroll
-        for (int r = 0; r < TM; ++r)
+                for (int r = 0; r < TM; ++r)
 #pragma unroll
-            for (int c = 0; c < TN; ++c) {
-                const int i = m0 + ty + TY * r, j = n0 + tx + TX * c;
-                if (i < M && j < N) st(i, j, acc[r][c]);
+                    for (int c = 0; c < TN; ++c) cv[r][c] = cpre[r][c];
+                if (it + 1 < total) fetch_c(fm0, fn0);
             }
+#pragma unroll
+            for (int r = 0; r < TM; ++r)
+#pragma unroll
+                for (int c = 0; c < TN; ++c) {
+                    int i, j;
+                    out_ij(r, c, i, j);
+                    i += m0;
+                    j += n0;
+                    if (i < M && j < N) {
+                        if constexpr (RMW)
+                            st(i, j, acc[r][c], cv[r][c]);
+                        else
+                            st(i, j, acc[r][c]);
+                    }
+                    acc[r][c] = 0.0;
+                }
+        }
+        if (it + 1 < total) put(cur ^ 1);
+        advance(cm0, cn0, ck0);
+        advance(fm0, fn0, fk0);
+        __syncthreads();
     }
-    __syncthreads();
+}
+
+template <class T, bool AMF, bool BKF, class LA, class LB, class ST>
+__device__ __forceinline__ void gemm(int M, int N, int K, LA la, LB lb, ST st, double *sm)
+{
+    gemm_core<T, AMF, BKF, false>(
+        M, N, K, la, lb, [](int, int) { return 0.0; }, st, sm);
+}
+
+/* C(i,j) <- st(i, j, sum_k a b, C(i,j)) with C read through lc */
+template <class T, bool AMF, bool BKF, class LA, class LB, class LC, class ST>
+__device__ __forceinline__ void gemm_rmw(int M, int N, int K, LA la, LB lb, LC lc, ST st,
+                                         double *sm)
+{
+    gemm_core<T, AMF, BKF, true>(M, N, K, la, lb, lc, st, sm);
 }
 
 /* Square-product dispatch by size: small lattices use 32x32 tiles. */
@@ -170,7 +312,7 @@ __device__ __forceinline__ void gemm_sq(int M, int N, int K, LA la, LB lb, ST st
     if (M <= 32 && N <= 32)
         gemm<TSm, AMF, BKF>(M, N, K, la, lb, st, sm);
     else
-        gemm<TSq, AMF, BKF>(M, N, K, la, lb, st, sm);
+        gemm<TMma, AMF, BKF>(M, N, K, la, lb, st, sm);
 }
 
 /* ------------------------------------------------------------ workspace */
@@ -192,8 +334,8 @@ struct Smem {
 __host__ __device__ inline size_t smem_doubles(int n, int kb)
 {
     const size_t qr = (size_t)n * QNB + (size_t)QNB * WCOLS + 2 * QNB * QNB + QNB;
-    const size_t ld = (size_t)kb + 1;
-    const size_t pr = 3 * (size_t)kb * ld + 2 * (size_t)kb;
+    (void)kb;
+    const size_t pr = 4 * (size_t)DQMC_MAX_KB * (DQMC_MAX_KB + 1) + DQMC_MAX_KB;
     const size_t un = qr > pr ? qr : pr;
     const size_t ints = (size_t)n + 2 * DQMC_MAX_KB + 8;
     return (size_t)GEMM_SMEM + 40 + 4 * (size_t)n + (ints + 1) / 2 + un + 8;
@@ -278,7 +420,7 @@ __device__ __noinline__ void apply_block(int m, int nb, const double *P, const d
         const int ncc = min(WCOLS, nc - cc);
         double *Xc = X + (size_t)cc * ldx;
         double *W = s.W;
-        gemm<TWide, false, true>(
+        gemm<TMmaWide, false, true>(
             nb, ncc, m, [=](int i, int k) { return vpan(P, m, k, i); },
             [=](int k, int j) { return Xc[k + (size_t)j * ldx]; },
             [=](int i, int j, double v) { W[i + j * QNB] = v; }, s.gsm);
@@ -303,10 +445,11 @@ __device__ __noinline__ void apply_block(int m, int nb, const double *P, const d
                 if (i < nb) W[i + j * QNB] = o[i];
         }
         __syncthreads();
-        gemm<TSq, true, true>(
+        gemm_rmw<TMma, true, true>(
             m, ncc, nb, [=](int i, int k) { return vpan(P, m, i, k); },
             [=](int k, int j) { return W[k + j * QNB]; },
-            [=](int i, int j, double v) { Xc[i + (size_t)j * ldx] -= v; }, s.gsm);
+            [=](int i, int j) { return Xc[i + (size_t)j * ldx]; },
+            [=](int i, int j, double v, double c) { Xc[i + (size_t)j * ldx] = c - v; }, s.gsm);
     }
 }
 
@@ -420,13 +563,12 @@ __device__ __noinline__ void trsm_upper(int n, const double *A, const double *Y,
     for (int i1 = n; i1 > 0; i1 -= QNB) {
         const int i0 = max(0, i1 - QNB), bs = i1 - i0;
         if (i1 < n) {
-            gemm<TWide, true, true>(
+            gemm_rmw<TMmaWide, true, true>(
                 bs, n, n - i1,
                 [=](int i, int k) { return A[(i0 + i) + (size_t)(i1 + k) * n]; },
                 [=](int k, int j) { return X[(i1 + k) + (size_t)j * n]; },
-                [=](int i, int j, double v) {
-                    X[(i0 + i) + (size_t)j * n] = Y[(i0 + i) + (size_t)j * n] - v;
-                },
+                [=](int i, int j) { return Y[(i0 + i) + (size_t)j * n]; },
+                [=](int i, int j, double v, double c) { X[(i0 + i) + (size_t)j * n] = c - v; },
                 s.gsm);
         } else {
             for (int e = threadIdx.x; e < bs * n; e += NT) {
@@ -578,10 +720,13 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
                          const signed char *fl, double v0, double v1, Scr w, Smem &s,
                          int *flag)
 {
-    for (int j = threadIdx.x; j < n; j += NT) s.vA[j] = checked_exp(u.ell[j], flag);
+    for (int j = threadIdx.x; j < n; j += NT) {
+        s.vA[j] = checked_exp(u.ell[j], flag);
+        if (B == nullptr) s.vD[j] = fl[j] > 0 ? v1 : v0;
+    }
     __syncthreads();
     const double *U = u.U;
-    double *eD = s.vA;
+    double *eD = s.vA, *vl = s.vD;
     double *M = w.m0;
     if (B != nullptr) {
         gemm_sq<true, true>(
@@ -591,9 +736,7 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
     } else {
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-            [=](int k, int j) {
-                return (fl[k] > 0 ? v1 : v0) * U[k + (size_t)j * n] * eD[j];
-            },
+            [=](int k, int j) { return vl[k] * U[k + (size_t)j * n] * eD[j]; },
             [=](int i, int j, double v) { M[i + (size_t)j * n] = v; }, s.gsm);
     }
     prepivot(n, M, w.m1, s, flag);
@@ -731,11 +874,15 @@ __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const dou
                            const double *expKinv, const signed char *fl, double v0,
                            double v1, double vi0, double vi1, Smem &s)
 {
+    double *vv = s.vA, *vi = s.vB;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        const bool up = fl[k] > 0;
+        vv[k] = up ? v1 : v0;
+        vi[k] = up ? vi1 : vi0;
+    }
     gemm_sq<true, true>(
         n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-        [=](int k, int j) {
-            return (fl[k] > 0 ? v1 : v0) * G[k + (size_t)j * n] * (fl[j] > 0 ? vi1 : vi0);
-        },
+        [=](int k, int j) { return vv[k] * G[k + (size_t)j * n] * vi[j]; },
         [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; }, s.gsm);
     gemm_sq<true, true>(
         n, n, n, [=](int i, int k) { return tmp[i + (size_t)k * n]; },
@@ -753,12 +900,15 @@ __device__ __noinline__ void bblock(int n, int l0, int len, const signed char *f
         first[e] = expK[e] * (f0[e / n] > 0 ? v1 : v0);
     __syncthreads();
     const double *src = first;
+    double *vv = s.vA;
     for (int p = 1; p < len; ++p) {
         double *dst = (p == len - 1) ? out : ((src == X) ? Y : X);
         const signed char *fp = field + (size_t)(l0 + p) * n;
+        __syncthreads();
+        for (int k = threadIdx.x; k < n; k += NT) vv[k] = fp[k] > 0 ? v1 : v0;
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-            [=](int k, int j) { return (fp[k] > 0 ? v1 : v0) * src[k + (size_t)j * n]; },
+            [=](int k, int j) { return vv[k] * src[k + (size_t)j * n]; },
             [=](int i, int j, double v) { dst[i + (size_t)j * n] = v; }, s.gsm);
         src = dst;
     }
@@ -783,4 +933,4 @@ __device__ __forceinline__ double rng_next(uint64_t *s)
     return (double)(res >> 11) * (1.0 / 9007199254740992.0);
 }
 
-}  // namespace dq
+}  // namespace DQMC_NS

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/dqmc_gpu.h"
+#include "dqmc_k2.h"
 #include "dqmc_kernels.cuh"
 
 namespace {
@@ -136,7 +137,8 @@ struct dqmc_engine {
     DqmcChainDev *dchains = nullptr;
     std::vector<DqmcChainDev> hdev;  /* host mirror: device pointers */
     int nbin = 0;
-    size_t smem = 0, msmem = 0;
+    size_t smem = 0, msmem = 0, smem2 = 0;
+    int per_sm = 1;           /* CTAs per SM of the sweep kernels (1 or 2) */
     bool prepared = false;
 };
 
@@ -280,7 +282,7 @@ int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
     c.stab = stab > 0 ? stab : 8;   /* green_stack_alloc default, src/green.c:172 */
     c.M = (L + c.stab - 1) / c.stab;
     int kb = e->desc.delay_rank;
-    if (kb <= 0) kb = n <= 256 ? 32 : 64;
+    if (kb <= 0) kb = 32;
     if (kb > DQMC_MAX_KB) kb = DQMC_MAX_KB;
     if (kb > n) kb = n;
     c.kb = kb;
@@ -394,8 +396,10 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
         off += rup((size_t)e->nbin * m.nq_perp * 8 + 8);
-        const size_t sm = dq::smem_doubles(n, c.kb) * 8;
+        const size_t sm = dq::smem_bytes(n, c.kb);
         if (sm > maxsmem) maxsmem = sm;
+        const size_t sm2 = dq2x::smem_bytes(n, c.kb);
+        if (sm2 > e->smem2) e->smem2 = sm2;
         if (n > maxn) maxn = n;
     }
     const size_t cstruct = off;
@@ -443,16 +447,19 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     e->smem = maxsmem;
     e->msmem = (size_t)2 * maxn * 8;
     if (e->smem > 227 * 1024) return set_err("shared memory need %zu B exceeds 227 KB", e->smem);
-    CU(cudaFuncSetAttribute(dq::k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)e->smem));
-    CU(cudaFuncSetAttribute(dq::k_init, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)e->smem));
-    CU(cudaFuncSetAttribute(dq::k_scratch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)e->smem));
-    CU(cudaFuncSetAttribute(dq::k_wrap, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)e->smem));
-    CU(cudaFuncSetAttribute(dq::k_measure, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)e->msmem));
+    CU(dq::set_attrs(e->smem, e->msmem));
+    /* Two chains per SM when the batch has more chains than SMs and two
+     * CTAs fit in shared memory: the second chain fills the first one's
+     * barrier and reduction latency. */
+    {
+        int dev = 0, nsm = 148;
+        CU(cudaGetDevice(&dev));
+        CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const bool fits2 = 2 * (e->smem2 + 1024) <= 228 * 1024;
+        const int want = e->desc.ctas_per_sm;
+        e->per_sm = (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 ? 2 : 1;
+        if (e->per_sm == 2) CU(dq2x::set_attrs(e->smem2, e->msmem));
+    }
     dq::k_init<<<(unsigned)nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(e->stream));
@@ -476,8 +483,11 @@ int dqmc_sweep(dqmc_engine *e, int nsweeps)
 {
     if (check_prepared(e, "dqmc_sweep")) return 1;
     if (nsweeps <= 0) return 0;
-    dq::k_sweep<<<(unsigned)e->chains.size(), DQMC_NT, e->smem, e->stream>>>(
-        e->dchains, e->dmodels, kflags(e), nsweeps);
+    const unsigned nc = (unsigned)e->chains.size();
+    if (e->per_sm == 2)
+        dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), nsweeps);
+    else
+        dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, kflags(e), nsweeps);
     CU(cudaGetLastError());
     return 0;
 }
@@ -488,9 +498,12 @@ int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
     if (bin < 0 || bin >= e->nbin) return set_err("dqmc_sweep_measure: bin %d out of range", bin);
     const unsigned nc = (unsigned)e->chains.size();
     for (int s = 0; s < nsweeps; ++s) {
-        dq::k_sweep<<<nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels,
-                                                         kflags(e) | dq::KF_MEASURE, 1);
-        dq::k_measure<<<nc, DQMC_NT, e->msmem, e->stream>>>(e->dchains, e->dmodels, bin);
+        const int f = kflags(e) | dq::KF_MEASURE;
+        if (e->per_sm == 2)
+            dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, f, 1);
+        else
+            dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, f, 1);
+        dq::launch_measure(nc, e->msmem, e->stream, e->dchains, e->dmodels, bin);
     }
     CU(cudaGetLastError());
     return 0;
@@ -571,6 +584,8 @@ int dqmc_read_counters(dqmc_engine *e, int chain, dqmc_chain_counters *out)
     out->scratch_drift_max = d.sdrift_max;
     out->scratch_drift_mean = d.sdrift_count ? d.sdrift_sum / (double)d.sdrift_count : 0.0;
     out->scratch_drift_samples = d.sdrift_count;
+    out->scratch_drift_max_tau = d.sdrift_max_tau;
+    out->scratch_drift_max_sweep = d.sdrift_max_sweep;
     for (int i = 0; i < 4; ++i) out->rng[i] = d.rng[i];
     return 0;
 }
@@ -709,7 +724,7 @@ int dqmc_udv_green(int device, int n, const double *U, const double *D, const do
     double *dG = ws + 3 * nn + twsz;
     int *ddet = (int *)(dG + nn);
     cudaError_t err = cudaMemcpy(dslot, slot.data(), usz * 8, cudaMemcpyHostToDevice);
-    const size_t sm = dq::smem_doubles(n, 1) * 8;
+    const size_t sm = dq::smem_bytes(n, 1);
     if (err == cudaSuccess)
         err = cudaFuncSetAttribute(dq::k_udv_green, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)sm);

@@ -2,7 +2,7 @@
 #pragma once
 #include "dqmc_device.cuh"
 
-namespace dq {
+namespace DQMC_NS {
 
 enum { KF_MEASURE = 1, KF_SDRIFT = 2, KF_STAB_DRIFT = 4 };
 
@@ -26,115 +26,150 @@ __device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
     return Scr{ch->w[0], ch->w[1], ch->w[2], ch->twall};
 }
 
-/* One site block of the delayed update (green.c:384-480 restated as a
- * submatrix update).  With S the block's sites and g = G[S,S] at block
- * start, every accepted flip keeps G_cur = G - X Gam Y, X = (I - G)[:,S],
- * Y = G[S,:], with Gam supported on the accepted sites only:
- *   x = (I + Gam g) e_a,  y^T = e_a^T (I - (I - g) Gam),  Gam += f x y^T,
- * and the block's own entries gt = G_cur[S,S] follow the rank-1 update of
- * green_delay_accept.  The ratio uses gt[a,a] exactly as
- * green_delay_ratio_N / green_ph_down_ratio_N (green.c:402-416).  After the
- * block, G -= (X Gam)[:,A] Y[A,:] is one rank-m GEMM.  Warp 0 runs the
- * proposals (one RNG draw per site, always consumed: dqmc.c:666-668). */
-__device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *G, signed char *fl,
-                           const DqmcModelDev &md, uint64_t *rng,
-                           unsigned long long *att, unsigned long long *acc,
-                           double *Zs, double *Ys, Smem &s, DqmcChainDev *ch,
-                           PhaseClock &pc)
+/* One site block of the delayed update (green.c:384-480, PH path).
+ *
+ * Proposals: warp 0, lane b holding column b of the block's current G~
+ * (gt[c][b] = G~[i0+c, i0+b]) in registers; the site loop is unrolled so
+ * every index is static.  The ratio uses gt[a][a] exactly as
+ * green_delay_ratio_N / green_ph_down_ratio_N (green.c:402-416), one RNG
+ * draw per site, always consumed (dqmc.c:666-668).  An accepted flip
+ * applies green_delay_accept's rank-1 update G~ -= fac (e_a - G~[:,a])
+ * G~[a,:] to the trailing block (rows and columns > a, the only entries
+ * later sites read) and records row a and column a of G~ at that moment.
+ *
+ * Flush: the reference's delayed vectors C[:,p] = fac_p u_p, V[:,p] = v_p
+ * satisfy u_p = e - G[:,i_p] + sum_{q<p} C[:,q] V[i_p,q] and v_p = G[i_p,:]
+ * - sum_{q<p} V[:,q] C[i_p,q]; with the recorded entries this is
+ * U (I - F Su) = E_A - G[:,A] and V (I + Sc) = G[A,:]^T (Su, Sc strictly
+ * upper m x m), so U and V come from two unit-triangular inverses, and
+ * G -= U F V^T is one rank-m GEMM (green_delay_flush, green.c:462-475). */
+__device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *G,
+                                        signed char *fl, const DqmcModelDev &md,
+                                        uint64_t *rng, unsigned long long *att,
+                                        unsigned long long *acc, double *Zs, double *Ys,
+                                        Smem &s, DqmcChainDev *ch, PhaseClock &pc)
 {
-    const int ld = kb + 1;
+    constexpr int KB = DQMC_MAX_KB;   /* 32: one lane per block column */
+    constexpr int LD = KB + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double *g0 = s.g0, *gt = s.gt, *gam = s.gam, *xs = s.xs, *colA = s.colA;
+    double *Rrow = s.g0;              /* [q*LD + b] = G~_q[a_q, b]      */
+    double *Ccol = Rrow + KB * LD;    /* [q*LD + c] = G~_q[c, a_q]      */
+    double *Tu = Ccol + KB * LD;      /* (I - F Su)^-1, row-major [q*LD+p] */
+    double *Tv = Tu + KB * LD;        /* (I + Sc)^-1                     */
+    double *facs = Tv + KB * LD;      /* fac_q                           */
     int *alist = s.iscr;
-    for (int e = threadIdx.x; e < kbs * kbs; e += NT) {
-        const int r = e % kbs, c = e / kbs;
-        const double v = G[(i0 + r) + (size_t)(i0 + c) * n];
-        g0[r + c * ld] = v;
-        gt[r + c * ld] = v;
-        gam[r + c * ld] = 0.0;
-    }
-    __syncthreads();
     if (warp == 0) {
+        double col[KB];
+        const bool mine = lane < kbs;
+#pragma unroll
+        for (int c = 0; c < KB; ++c)
+            col[c] = (mine && c < kbs) ? G[(i0 + c) + (size_t)(i0 + lane) * n] : 0.0;
+        int fvl = mine ? (int)fl[i0 + lane] : 1;
+        const double Nu0 = md.Nup[0], Nu1 = md.Nup[1], Nd0 = md.Ndn[0], Nd1 = md.Ndn[1];
+        uint64_t r4[4] = {0, 0, 0, 0};
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r4[q] = rng[q];
+        }
+        unsigned long long nacc = 0;
         int m = 0;
-        for (int a = 0; a < kbs; ++a) {
-            const signed char sv = fl[i0 + a];
-            const int si = sv > 0;
-            const double Nu = md.Nup[si], Nd = md.Ndn[si];
-            const double gii = gt[a + a * ld];
-            const double Ru = 1.0 + (1.0 - gii) * Nu;
-            const double Rd = 1.0 + gii * Nd;
-            const double R = Ru * Rd;
-            double u = 0.0;
-            if (lane == 0) {
-                u = rng_next(rng);
-                ++*att;
-            }
-            u = __shfl_sync(FULL, u, 0);
-            if (u < fabs(R)) {
-                const double fac = Nu / Ru;
-                double yv[2], ra[2];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int b = lane + 32 * h;
-                    yv[h] = 0.0;
-                    ra[h] = 0.0;
-                    if (b < kbs) {
-                        double x = (b == a) ? 1.0 : 0.0, y = x;
-                        for (int c = 0; c < kbs; ++c) {
-                            x += gam[b + c * ld] * g0[c + a * ld];
-                            y -= ((c == a) ? 1.0 - g0[a + c * ld] : -g0[a + c * ld]) *
-                                 gam[c + b * ld];
-                        }
-                        xs[b] = x;
-                        colA[b] = gt[b + a * ld];
-                        yv[h] = y;
-                        ra[h] = gt[a + b * ld];
-                    }
-                }
-                __syncwarp();
+        for (int a = 0; a < KB; ++a) {
+            if (a < kbs) {
+                const int sv = __shfl_sync(FULL, fvl, a);
+                const double gii = __shfl_sync(FULL, col[a], a);
+                const bool up = sv > 0;
+                const double Nu = up ? Nu1 : Nu0, Nd = up ? Nd1 : Nd0;
+                const double Ru = 1.0 + (1.0 - gii) * Nu;
+                const double Rd = 1.0 + gii * Nd;
+                const double R = Ru * Rd;
+                double u = 0.0;
+                if (lane == 0) u = rng_next(r4);
+                u = __shfl_sync(FULL, u, 0);
+                if (u < fabs(R)) {
+                    const double fac = Nu / Ru;
+                    const double ra = col[a];        /* G~[a, lane] */
+                    double mycol = 0.0;              /* G~[lane, a] */
+                    const double fra = fac * ra;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int b = lane + 32 * h;
-                    if (b < kbs) {
-                        const double fy = fac * yv[h], fr = fac * ra[h];
-                        for (int c = 0; c < kbs; ++c) {
-                            gam[c + b * ld] += xs[c] * fy;
-                            gt[c + b * ld] -= ((c == a) ? 1.0 - colA[c] : -colA[c]) * fr;
-                        }
+                    for (int c = a + 1; c < KB; ++c) {
+                        const double vc = __shfl_sync(FULL, col[c], a);
+                        if (c == lane) mycol = vc;
+                        col[c] = fma(vc, fra, col[c]);
                     }
+                    Rrow[m * LD + lane] = ra;
+                    Ccol[m * LD + lane] = mycol;
+                    if (lane == a) fvl = -sv;
+                    if (lane == 0) {
+                        facs[m] = fac;
+                        alist[m] = a;
+                        ++nacc;
+                    }
+                    ++m;
                 }
-                __syncwarp();
-                if (lane == 0) {
-                    fl[i0 + a] = (signed char)(-sv);
-                    ++*acc;
-                    alist[m] = a;
-                }
-                ++m;
             }
         }
-        if (lane == 0) s.iscr[2 * DQMC_MAX_KB] = m;
+        if (mine) fl[i0 + lane] = (signed char)fvl;
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) rng[q] = r4[q];
+            *att += (unsigned long long)kbs;
+            *acc += nacc;
+            s.iscr[2 * DQMC_MAX_KB] = m;
+        }
     }
     __syncthreads();
     pc.charge(ch, DQMC_PH_PROPOSE);
     const int m = s.iscr[2 * DQMC_MAX_KB];
     if (m == 0) return;
-    /* Z = X[:,A] Gam[A,A] and Y[A,:] from G before it changes */
+    /* Tu = (I - F Su)^-1 (warp 0), Tv = (I + Sc)^-1 (warp 1); lane q owns
+     * row q.  Su[r][p] = V[i_p, r] = Rrow[r][a_p], Sc[r][p] = C[i_p, r] =
+     * -fac_r Ccol[r][a_p], both for r < p. */
+    if (warp < 2) {
+        double xr[KB];
+        const int q = lane;
+#pragma unroll
+        for (int p = 0; p < KB; ++p) {
+            double v = 0.0;
+            if (p < m && q <= p) {
+                v = (q == p) ? 1.0 : 0.0;
+                const int ap = alist[p];
+#pragma unroll
+                for (int r = 0; r < p; ++r) {
+                    if (r >= q) {
+                        const double nrp = (warp == 0) ? -facs[r] * Rrow[r * LD + ap]
+                                                       : -facs[r] * Ccol[r * LD + ap];
+                        v -= xr[r] * nrp;
+                    }
+                }
+            }
+            xr[p] = v;
+        }
+        double *T = (warp == 0) ? Tu : Tv;
+#pragma unroll
+        for (int p = 0; p < KB; ++p)
+            if (p < m) T[q * LD + p] = xr[p];
+    }
+    __syncthreads();
+    /* Zs = (E_A - G[:,A]) Tu F  (n x m),  Ys = Tv^T G[A,:]  (m x n) */
     gemm_sq<true, true>(
         n, m, m,
         [=](int i, int k) {
             const int col = i0 + alist[k];
             return (i == col ? 1.0 : 0.0) - G[i + (size_t)col * n];
         },
-        [=](int k, int j) { return gam[alist[k] + alist[j] * ld]; },
-        [=](int i, int j, double v) { Zs[i + (size_t)j * n] = v; }, s.gsm);
-    for (int e = threadIdx.x; e < m * n; e += NT) {
-        const int q = e % m, c = e / m;
-        Ys[q + (size_t)c * kb] = G[(i0 + alist[q]) + (size_t)c * n];
-    }
-    gemm_sq<true, true>(
+        [=](int k, int j) { return Tu[k * LD + j]; },
+        [=](int i, int j, double v) { Zs[i + (size_t)j * n] = v * facs[j]; }, s.gsm);
+    gemm<TMmaWide, false, true>(
+        m, n, m, [=](int i, int k) { return Tv[k * LD + i]; },
+        [=](int k, int j) { return G[(i0 + alist[k]) + (size_t)j * n]; },
+        [=](int i, int j, double v) { Ys[i + (size_t)j * kb] = v; }, s.gsm);
+    /* G -= Zs Ys */
+    gemm_rmw<TMma, true, true>(
         n, n, m, [=](int i, int k) { return Zs[i + (size_t)k * n]; },
         [=](int k, int j) { return Ys[k + (size_t)j * kb]; },
-        [=](int i, int j, double v) { G[i + (size_t)j * n] -= v; }, s.gsm);
+        [=](int i, int j) { return G[i + (size_t)j * n]; },
+        [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
     pc.charge(ch, DQMC_PH_FLUSH);
 }
 
@@ -231,7 +266,11 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
             if (threadIdx.x == 0) {
                 ch->sdrift_count++;
                 ch->sdrift_sum += d;
-                if (d > ch->sdrift_max || ch->sdrift_count == 1) ch->sdrift_max = d;
+                if (d > ch->sdrift_max || ch->sdrift_count == 1) {
+                    ch->sdrift_max = d;
+                    ch->sdrift_max_tau = tau;
+                    ch->sdrift_max_sweep = ch->sweeps;
+                }
             }
             pc.charge(ch, DQMC_PH_SDRIFT);
         }
@@ -271,7 +310,7 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
     return true;
 }
 
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, DQMC_MINB)
     k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps)
 {
     extern __shared__ double smraw[];
@@ -314,7 +353,7 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 /* G from scratch at l0 = 0 for every chain (dqmc_init_modes, dqmc.c:466-483). */
-__global__ void __launch_bounds__(NT, 1) k_init(DqmcChainDev *chains, const DqmcModelDev *models)
+__global__ void __launch_bounds__(NT, DQMC_MINB) k_init(DqmcChainDev *chains, const DqmcModelDev *models)
 {
     extern __shared__ double smraw[];
     __shared__ int flag;
@@ -333,7 +372,7 @@ __global__ void __launch_bounds__(NT, 1) k_init(DqmcChainDev *chains, const Dqmc
 }
 
 /* Test kernels: rebuild from scratch into out; wrap a caller G. */
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, DQMC_MINB)
     k_scratch(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l0, double *out,
               int *det)
 {
@@ -348,7 +387,7 @@ __global__ void __launch_bounds__(NT, 1)
     if (threadIdx.x == 0) *det = flag ? 0 : ds;
 }
 
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, DQMC_MINB)
     k_wrap(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l, double *Gio)
 {
     extern __shared__ double smraw[];
@@ -361,7 +400,7 @@ __global__ void __launch_bounds__(NT, 1)
 }
 
 /* Caller UDV -> G (fixture parity).  ws: 4 n*n scratch + tw + UDV slot. */
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, DQMC_MINB)
     k_udv_green(int n, double *slot, double *ws, double *G, int *det)
 {
     extern __shared__ double smraw[];
@@ -482,4 +521,42 @@ __global__ void __launch_bounds__(NT)
     pc.charge(ch, DQMC_PH_MEASURE);
 }
 
-}  // namespace dq
+/* ---------------------------------------------------------- launchers */
+inline size_t smem_bytes(int n, int kb) { return smem_doubles(n, kb) * sizeof(double); }
+
+inline cudaError_t set_attrs(size_t smem, size_t msmem)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_scratch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_wrap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_measure, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)msmem);
+    return e;
+}
+
+inline void launch_sweep(unsigned nc, size_t smem, cudaStream_t st, DqmcChainDev *c,
+                         const DqmcModelDev *m, int flags, int nsweeps)
+{
+    k_sweep<<<nc, NT, smem, st>>>(c, m, flags, nsweeps);
+}
+
+inline void launch_measure(unsigned nc, size_t msmem, cudaStream_t st, DqmcChainDev *c,
+                           const DqmcModelDev *m, int bin)
+{
+    k_measure<<<nc, NT, msmem, st>>>(c, m, bin);
+}
+
+inline void launch_init(unsigned nc, size_t smem, cudaStream_t st, DqmcChainDev *c,
+                        const DqmcModelDev *m)
+{
+    k_init<<<nc, NT, smem, st>>>(c, m);
+}
+
+}  // namespace DQMC_NS

@@ -16,7 +16,7 @@ import os
 import numpy as np
 
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG, "libdqmc_b200.so")
+LIB_PATH = os.environ.get("DQMC_B200_LIB") or os.path.join(PKG, "libdqmc_b200.so")
 
 PREC_FP64, PREC_MIXED = 0, 1
 DRIFT_STAB, DRIFT_SCRATCH = 1, 2
@@ -34,7 +34,7 @@ _bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
 class Desc(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int),
                 ("delay_rank", C.c_int), ("drift", C.c_int),
-                ("reserved", C.c_int * 8)]
+                ("ctas_per_sm", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class Counters(C.Structure):
@@ -45,10 +45,12 @@ class Counters(C.Structure):
                 ("scratch_drift_max", C.c_double),
                 ("scratch_drift_mean", C.c_double),
                 ("scratch_drift_samples", C.c_ulonglong),
+                ("scratch_drift_max_tau", C.c_int), ("pad2", C.c_int),
+                ("scratch_drift_max_sweep", C.c_ulonglong),
                 ("rng", C.c_uint64 * 4)]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pad", "rng")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pad", "pad2", "rng")}
         d["rng"] = np.array(list(self.rng), dtype=np.uint64)
         return d
 
@@ -181,11 +183,12 @@ class Engine:
     """A batch of chains on one GPU (the C ABI's dqmc_engine)."""
 
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
-                 drift=DRIFT_STAB):
+                 drift=DRIFT_STAB, ctas_per_sm=0):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
         d.device, d.precision, d.delay_rank, d.drift = device, precision, delay_rank, drift
+        d.ctas_per_sm = ctas_per_sm
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
             raise DqmcError(L.dqmc_last_error().decode())

@@ -1,0 +1,119 @@
+"""End-to-end: the dqmc_gpu driver on a reference input file.
+
+With the same seeds the GPU chains flip exactly the same fields as the
+reference, so observables.dat, szz.dat, sperp.dat and the consistency file
+agree with the reference program to rounding (compared at 1e-6 relative
+after the reference's own %.6g-%.8g printing), and with the CPU oracle.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG, ROOT
+
+pytestmark = pytest.mark.gpu
+
+INPUT = """lattice=chain
+Lx=4
+pbc=1
+t=-1.0
+U=4.0
+dtau=0.1
+beta_list=0.5,1.0,2.0
+nwarm=20
+nmeas=40
+nbin=4
+nrep=2
+seed=1
+szz_q=all
+sperp_q=all
+spin_consistency_file=consistency.dat
+"""
+
+EXE = os.path.join(PKG, "dqmc_gpu")
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "dqmc")
+
+
+def run(exe, d):
+    (d / "input.txt").write_text(INPUT)
+    r = subprocess.run([exe, "input.txt"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+def table(path):
+    rows = [l.split() for l in open(path) if l.strip() and not l.startswith("#")]
+    return np.array([[float(x) for x in r] for r in rows])
+
+
+def oracle_rows(oracle):
+    """The same run through the CPU oracle: bins, ratios and jackknife."""
+    beta, nwarm, nmeas, nbin, nrep, U = [0.5, 1.0, 2.0], 20, 40, 4, 2, 4.0
+    rows = []
+    for b, bt in enumerate(beta):
+        L = int(round(bt / 0.1))
+        series = [[] for _ in range(7)]
+        for r in range(nrep):
+            seed = oracle.replica_seed(1, b, r)
+            ch = oracle.chain(0, 4, 1, U, 0.1, L, 8, seed)
+            ch.sweep(nwarm)
+            a0 = ch.state()
+            for _ in range(nbin):
+                acc = np.zeros(6)
+                att0, acc0 = a0["attempts"], a0["accepted"]
+                for _ in range(nmeas // nbin):
+                    ch.sweep(1)
+                    m, _, _ = oracle.measure(ch, 0)
+                    E, ntot, D = m[0], m[3], m[4]
+                    acc += [E, E - U / 2 * ntot, E - 0.5 * U * ntot + 0.25 * U * 4, ntot, D, 1.0]
+                a0 = ch.state()
+                cnt = nmeas // nbin
+                vals = list(acc[:5] / acc[5]) + [acc[5] / cnt,
+                                                 (a0["accepted"] - acc0) / (a0["attempts"] - att0)]
+                for k in range(7):
+                    series[k].append(vals[k])
+        out = [1.0 / (L * 0.1)]
+        for k, s in enumerate(series):
+            m, e = oracle.jackknife(np.array(s))
+            out += [m] if k == 5 else [m, e]
+        rows.append(out)
+    return np.array(rows)
+
+
+def test_cli_matches_reference_and_oracle(tmp_path, oracle):
+    gdir = tmp_path / "gpu"
+    gdir.mkdir()
+    run(EXE, gdir)
+    obs = table(gdir / "observables.dat")
+    assert obs.shape == (3, 14)
+    # 14-column header and row format of the reference (src/main.c:909, 259-262)
+    head = open(gdir / "observables.dat").read().splitlines()
+    assert head[1].startswith("# T  E_hub dE_hub  E_gc dE_gc")
+    want = oracle_rows(oracle)
+    np.testing.assert_allclose(obs[:, [0, 1, 3, 5, 7, 9, 11, 12]],
+                               want[:, [0, 1, 3, 5, 7, 9, 11, 12]], rtol=1e-6, atol=1e-9)
+    for name in ("szz.dat", "sperp.dat", "consistency.dat"):
+        t = table(gdir / name)
+        assert t.shape == (3 * 4, 12)
+    if os.path.exists(REF_EXE):
+        rdir = tmp_path / "ref"
+        rdir.mkdir()
+        run(REF_EXE, rdir)
+        for name in ("observables.dat", "szz.dat", "sperp.dat", "consistency.dat"):
+            a, b = table(gdir / name), table(rdir / name)
+            assert a.shape == b.shape
+            np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-9, err_msg=name)
+        ha = [l for l in open(gdir / "szz.dat") if l.startswith("#")]
+        hb = [l for l in open(rdir / "szz.dat") if l.startswith("#")]
+        assert ha == hb
+
+
+def test_cli_rejects_like_reference(tmp_path):
+    (tmp_path / "input.txt").write_text("lattice=chain\nLx=5\npbc=1\n")
+    r = subprocess.run([EXE, "input.txt"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "non-bipartite" in r.stderr
+    (tmp_path / "input.txt").write_text("beta_list=0.55\ndtau=0.1\nnmeas=4\nnbin=2\n")
+    r = subprocess.run([EXE, "input.txt"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "not a multiple of dtau" in r.stderr

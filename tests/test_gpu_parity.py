@@ -128,10 +128,11 @@ def test_random_configs_vs_oracle(oracle, Lx, U, L, stab, seed, kb):
         assert abs(zz[s, 0] - szz[0]) < 10 * tol and abs(pp[s, 0] - sperp[0]) < 10 * tol
 
 
-def test_batched_uneven_chains_match_single(oracle):
+@pytest.mark.parametrize("per_sm", [1, 2])
+def test_batched_uneven_chains_match_single(oracle, per_sm):
     """Chains of different n and L in one launch give the same results as
-    the oracle run one by one."""
-    eng = dq.Engine()
+    the oracle run one by one (one or two chains resident per SM)."""
+    eng = dq.Engine(ctas_per_sm=per_sm)
     specs = [(4, 4.0, 20, 8, 1), (6, 2.0, 30, 10, 2), (8, 6.0, 12, 4, 3), (4, 4.0, 40, 8, 4)]
     for (Lx, U, L, stab, seed) in specs:
         T, bp = dq.square_lattice(Lx, Lx)
