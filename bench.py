@@ -1,0 +1,429 @@
+#!/usr/bin/env python3
+"""Benchmark of the BSS determinant-QMC sweep on one B200 (or N, as replicas).
+
+Workload (the lattice the headline metric is quoted on): 16x16 periodic
+square lattice, t=-1, U=4, dtau=0.1, beta=8 (L=80), stabilization every 8
+slices, delayed-update site blocks of 32, many independent replica chains
+(seeds replica_seed(11, 0, r), src/replica.c:17-34) advancing together.
+A step is one forward sweep of every chain followed by the fused
+equal-time measurement.  value = whole-job field updates/s
+(chains * n * L per step / device time, max over ranks).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--chains B]
+  python bench.py --impl reference ...   # the reference CPU code, host cores
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "sai-qmc_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = ("field updates/s, 16x16 U=4 β=8: batched mixed vs plain FP64 GPU, "
+          "max|ΔG|≤1e-8")
+UNIT = "field updates/s"
+LX, U, DTAU, BETA, STAB, KB, SEED = 16, 4.0, 0.1, 8.0, 8, 32, 11
+N_SITES = LX * LX
+L_SLICES = int(round(BETA / DTAU))
+L2_BYTES = 126 * 2**20
+
+
+def workload_name(chains):
+    return (f"16x16 square pbc, U=4, dtau=0.1, beta=8 (L=80), stab=8, delay rank 32, "
+            f"{chains} replica chains per GPU, seeds replica_seed(11, 0, r)")
+
+
+# --------------------------------------------------------------- helpers
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def flops_per_chain_sweep(n, L, s, accepted):
+    """Floating-point work of one forward sweep of one chain as this engine
+    performs it (multiply-adds counted as 2 flops, triangular factors at
+    their algorithmic cost):
+      wrap            2 GEMMs per slice                   4 n^3 L
+      flush           rank-m updates of G                 2 n^2 * accepted
+      B-block         (len-1) GEMMs per block, left pass  2 n^3 (L - M)
+      suffix rmul     GEMM + QR + form Q + GEMM           (4 + 8/3) n^3 (M-1)
+      left lmul       GEMM + QR + form Q + triangular     (3 + 8/3) n^3 M
+      combine         2 GEMM + QR + form Q + triangular   (5 + 8/3) n^3 (M-1)
+      G from UDV      QR + apply Q^T + triangular solve   (4/3 + 2 + 1) n^3 M
+    """
+    M = (L + s - 1) // s
+    n3 = float(n) ** 3
+    return (4 * n3 * L + 2.0 * n * n * accepted + 2 * n3 * (L - M)
+            + (4 + 8 / 3) * n3 * (M - 1) + (3 + 8 / 3) * n3 * M
+            + (5 + 8 / 3) * n3 * (M - 1) + (4 / 3 + 3) * n3 * M)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9 or parts[0] != str(self.idx):
+                    continue
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        mhz = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(mhz) if mhz else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "power_w_max": max(float(r[3]) for r in rows
+                                   if r[3].replace(".", "").isdigit()) if rows else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+def physical_gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def fp64_gemm_peak_tflops():
+    """cuBLAS DGEMM (torch.matmul, float64, 8192^3), best of 5: the measured
+    FP64 tensor-core ceiling the sweep kernel's roofline is quoted against."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def traffic_per_chain_sweep():
+    """DRAM bytes per chain-sweep of the sweep kernel from the committed ncu
+    summary (profiles/), or None when no capture has been summarized."""
+    path = os.path.join(ROOT, "profiles", "k_sweep_16x16_ncu.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_chain_sweep:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+# ------------------------------------------------------ reference CPU arm
+def reference_cpu(steps, warmup, chains=None):
+    """The reference's own sweep (dqmc_sweep, src/dqmc.c:952) on the host
+    cores: one chain per core, each step one sweep of every chain, threads
+    released from the GIL inside the C calls.  Falls back to the oracle
+    restatement when the reference could not be compiled."""
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    from oracle.bind import LAT_SQUARE, Oracle, Reference
+    cores = len(os.sched_getaffinity(0))
+    chains = chains or cores
+    if Reference.available():
+        lib, kind = Reference(), "reference"
+    else:
+        lib, kind = Oracle(), "port"
+    seeds = [lib.replica_seed(SEED, 0, r) for r in range(chains)]
+    objs = [None] * chains
+
+    def make(i):
+        objs[i] = lib.chain(LAT_SQUARE, LX, LX, U, DTAU, L_SLICES, STAB, seeds[i])
+
+    def parallel(fn):
+        th = [threading.Thread(target=fn, args=(i,)) for i in range(chains)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+
+    parallel(make)
+    for _ in range(warmup):
+        parallel(lambda i: objs[i].sweep(1))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        parallel(lambda i: objs[i].sweep(1))
+    dt = time.perf_counter() - t0
+    for o in objs:
+        o.free()
+    value = chains * N_SITES * L_SLICES * steps / dt
+    sample = (f"{chains} chains x {steps} sweeps of the 16x16 U=4 beta=8 stab=8 workload, "
+              f"one chain per host core, {dt:.1f} s wall")
+    return {"value": value, "unit": UNIT, "cores": min(cores, chains), "kind": kind,
+            "sample": sample, "seconds": dt}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    r = reference_cpu(args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * r["seconds"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(r["cores"]) + " (CPU: one chain per core)",
+                   "chains": r["cores"]},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"],
+                         "kind": r["kind"], "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ GPU arm
+def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB):
+    T, bp = dq.square_lattice(LX, LX)
+    eng = dq.Engine(device=device, precision=precision, delay_rank=delay_rank)
+    m = eng.add_model(T, bp, U, DTAU, LX, LX, szz="af", sperp="af")
+    for r in range(chains):
+        eng.add_chain(m, L_SLICES, STAB, dq_replica_seed(SEED, 0, seed0 + r))
+    return eng
+
+
+def dq_replica_seed(base, b, r):
+    """replica_seed (src/replica.c:17-34), as dqmc_host computes it."""
+    import ctypes as C
+
+    import dqmc_b200 as dq
+    lib = dq.lib()
+    lib.dqmc_replica_seed.restype = C.c_ulonglong
+    lib.dqmc_replica_seed.argtypes = [C.c_ulonglong, C.c_int, C.c_int]
+    return lib.dqmc_replica_seed(base, b, r)
+
+
+def e2e_run(steps, warmup, chains, precision):
+    """The user-facing call end to end: dqmc_host_run on an input file for the
+    same workload (host parsing, model exponential, uploads of the model and
+    of every chain's field, initial G, warm-up and measured sweeps, read-back
+    of the bins, jackknife and output files), wall-clock timed."""
+    import ctypes as C
+
+    import dqmc_b200 as dq
+    lib = dq.lib()
+    lib.dqmc_host_run.argtypes = [C.c_char_p]
+    nbin = max(2, steps)
+    nmeas = nbin * max(1, math.ceil(steps / nbin))
+    text = (f"lattice=square\nLx={LX}\nLy={LX}\nbc=periodic\nt=-1.0\nU={U}\ndtau={DTAU}\n"
+            f"beta_list={BETA}\nstab={STAB}\nnwarm={warmup}\nnmeas={nmeas}\nnbin={nbin}\n"
+            f"nrep={chains}\nseed={SEED}\ndelay_rank={KB}\nprecision={precision}\n"
+            f"replica_log=none\nszz_q=af\nsperp_q=af\n")
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "input.txt"), "w") as f:
+            f.write(text)
+        os.chdir(d)
+        try:
+            devnull = os.open(os.devnull, os.O_WRONLY)
+            saved = os.dup(1)
+            os.dup2(devnull, 1)
+            t0 = time.perf_counter()
+            rc = lib.dqmc_host_run(b"input.txt")
+            dt = time.perf_counter() - t0
+            os.dup2(saved, 1)
+            os.close(devnull)
+            os.close(saved)
+        finally:
+            os.chdir(cwd)
+    if rc != 0:
+        return None
+    sweeps = warmup + nmeas
+    h2d = 3 * N_SITES * N_SITES * 8 + chains * (L_SLICES * N_SITES + 32)
+    d2h = chains * nbin * (9 + 2) * 8
+    return {"value": chains * N_SITES * L_SLICES * sweeps / dt, "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d / sweeps), "d2h_bytes_per_step": int(d2h / sweeps),
+            "seconds": dt, "sweeps": sweeps,
+            "note": "whole dqmc_gpu job (setup, uploads, initial G, warm-up and measured "
+                    "sweeps, read-back, outputs) through dqmc_host_run; bytes are the job's "
+                    "host<->device copies divided by its sweeps"}
+
+
+def run_gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import dqmc_b200 as dq
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    os.environ.setdefault("CUDA_DEVICE_ORDER", "PCI_BUS_ID")
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    props = torch.cuda.get_device_properties(local)
+    chains = args.chains or 2 * props.multi_processor_count
+    precision = dq.PREC_MIXED if args.precision == "mixed" else dq.PREC_FP64
+    eng = make_engine(dq, chains, rank * chains, precision, device=local)
+    nbin = max(1, args.steps)
+    eng.prepare(nbin)
+    for w in range(args.warmup):
+        eng.sweep_measure(1, 0)
+    eng.sync()
+    eng.clear_bins()
+    c0 = [eng.counters(c) for c in range(chains)]
+
+    def barrier():
+        if world > 1:
+            t = torch.zeros(1, device="cuda")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    sampler = ClockSampler(physical_gpu_index(local))
+    barrier()
+    eng.sync()
+    eng.kernel_timing(True)
+    eng.mark(0)
+    for k in range(args.steps):
+        eng.sweep_measure(1, k % nbin)
+    eng.mark(1)
+    ms = eng.elapsed_ms()
+    eng.sync()
+    barrier()
+    clocks = sampler.stop()
+    sweep_ms, nsweep, meas_ms, nmeas = eng.kernel_times()
+    eng.kernel_timing(False)
+    c1 = [eng.counters(c) for c in range(chains)]
+    status_bad = sum(1 for c in c1 if c["status"] != 0)
+    accepted = sum(c1[i]["accepted"] - c0[i]["accepted"] for i in range(chains))
+    attempts = sum(c1[i]["attempts"] - c0[i]["attempts"] for i in range(chains))
+    drift = max(c["drift_max"] for c in c1)
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * chains * N_SITES * L_SLICES * args.steps / (ms_max * 1e-3)
+    eng.close()
+
+    if rank == 0:
+        acc_per_chain_sweep = accepted / max(1, chains * args.steps)
+        flops_launch = chains * flops_per_chain_sweep(N_SITES, L_SLICES, STAB, acc_per_chain_sweep)
+        avg_launch = sweep_ms / max(1, nsweep)
+        achieved = flops_launch / (avg_launch * 1e-3) / 1e12
+        try:
+            peak = fp64_gemm_peak_tflops()
+            peak_src = "measured: cuBLAS DGEMM 8192^3 on this GPU (bench.py)"
+        except Exception as exc:  # pragma: no cover
+            peak, peak_src = 40.0, f"nominal FP64 (DGEMM probe failed: {exc})"
+        tb = traffic_per_chain_sweep()
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": tb * chains if tb else None,
+                    "kernel": "k_sweep (one launch = one sweep of every chain)",
+                    "flops_per_launch": flops_launch, "avg_launch_ms": avg_launch,
+                    "peak_source": peak_src}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == dq.PREC_FP64 else "f64 (split i8 wrap/flush)",
+            "data": "synthetic: HS fields drawn from each chain's own xoshiro256** stream",
+            "config": {"workload": workload_name(chains), "chains_per_gpu": chains,
+                       "n": N_SITES, "L": L_SLICES, "stab": STAB, "delay_rank": KB,
+                       "precision": args.precision,
+                       "l2": f"inputs larger than L2: {chains} chains x ~21 MB resident "
+                             f"state >> {L2_BYTES // 2**20} MB L2",
+                       "parallelism": f"replicas x{world} (no collective on the data path)"},
+            "roofline": roofline,
+            "gpu_launches": nsweep + nmeas,
+            "clocks": clocks,
+            "acceptance": accepted / max(1, attempts),
+            "drift_max": drift,
+            "chains_failed": status_bad,
+            "measure_ms_per_step": meas_ms / max(1, nmeas),
+        }
+        if not args.no_single_chain and world == 1:
+            e1 = make_engine(dq, 1, 0, precision)
+            e1.prepare(1)
+            e1.sweep(1)
+            e1.sync()
+            e1.mark(0)
+            e1.sweep(2)
+            e1.mark(1)
+            t1 = e1.elapsed_ms() / 2
+            e1.close()
+            line["single_chain"] = {"value": N_SITES * L_SLICES / (t1 * 1e-3), "unit": UNIT,
+                                    "ms_per_sweep": t1}
+        if not args.no_e2e and world == 1:
+            line["e2e"] = e2e_run(args.steps, args.warmup, chains, args.precision)
+        if not args.no_cpu_baseline and world == 1:
+            cb = reference_cpu(2, 0)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--chains", type=int, default=0, help="chains per GPU (0: 2 x SMs)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-single-chain", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)   # at least three untimed steps
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -121,6 +121,18 @@ int dqmc_sweep(dqmc_engine *e, int nsweeps);
  * (replica_result_add_sample, src/replica.c:240-269). */
 int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin);
 
+/* CUDA-event timing on the engine's stream (the stream every kernel of
+ * the engine runs on).  dqmc_kernel_timing(e, 1) records an event pair
+ * around every later sweep-kernel and measurement-kernel launch;
+ * dqmc_kernel_times waits and returns the summed milliseconds and launch
+ * counts since.  dqmc_timer_mark(e, 0|1) records a start/stop event;
+ * dqmc_timer_elapsed waits for the stop event and returns the interval. */
+int dqmc_kernel_timing(dqmc_engine *e, int enable);
+int dqmc_kernel_times(dqmc_engine *e, double *sweep_ms, int *sweep_launches,
+                      double *measure_ms, int *measure_launches);
+int dqmc_timer_mark(dqmc_engine *e, int which);
+int dqmc_timer_elapsed(dqmc_engine *e, double *ms);
+
 /* Waits for queued work; returns nonzero on a CUDA error. */
 int dqmc_synchronize(dqmc_engine *e);
 

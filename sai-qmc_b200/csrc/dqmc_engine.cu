@@ -140,7 +140,32 @@ struct dqmc_engine {
     size_t smem = 0, msmem = 0, smem2 = 0;
     int per_sm = 1;           /* CTAs per SM of the sweep kernels (1 or 2) */
     bool prepared = false;
+    /* per-launch CUDA events (kind 0 = sweep kernel, 1 = measurement) */
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_kind;
+    cudaEvent_t mark[2] = {nullptr, nullptr};
 };
+
+static void ev_begin(dqmc_engine *e, int kind)
+{
+    if (!e->timing) return;
+    cudaEvent_t a;
+    cudaEventCreate(&a);
+    cudaEventRecord(a, e->stream);
+    e->ev.push_back(a);
+    e->ev_kind.push_back(kind);
+}
+
+static void ev_end(dqmc_engine *e)
+{
+    if (!e->timing) return;
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, e->stream);
+    e->ev.push_back(b);
+    e->ev_kind.push_back(-1);
+}
 
 extern "C" {
 
@@ -208,6 +233,9 @@ void dqmc_engine_destroy(dqmc_engine *e)
     if (!e) return;
     cudaSetDevice(e->desc.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
+    for (cudaEvent_t v : e->ev) cudaEventDestroy(v);
+    for (cudaEvent_t v : e->mark)
+        if (v) cudaEventDestroy(v);
     cudaFree(e->dmod);
     cudaFree(e->darena);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -484,10 +512,12 @@ int dqmc_sweep(dqmc_engine *e, int nsweeps)
     if (check_prepared(e, "dqmc_sweep")) return 1;
     if (nsweeps <= 0) return 0;
     const unsigned nc = (unsigned)e->chains.size();
+    ev_begin(e, 0);
     if (e->per_sm == 2)
         dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), nsweeps);
     else
         dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, kflags(e), nsweeps);
+    ev_end(e);
     CU(cudaGetLastError());
     return 0;
 }
@@ -499,13 +529,70 @@ int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
     const unsigned nc = (unsigned)e->chains.size();
     for (int s = 0; s < nsweeps; ++s) {
         const int f = kflags(e) | dq::KF_MEASURE;
+        ev_begin(e, 0);
         if (e->per_sm == 2)
             dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, f, 1);
         else
             dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, f, 1);
+        ev_end(e);
+        ev_begin(e, 1);
         dq::launch_measure(nc, e->msmem, e->stream, e->dchains, e->dmodels, bin);
+        ev_end(e);
     }
     CU(cudaGetLastError());
+    return 0;
+}
+
+int dqmc_kernel_timing(dqmc_engine *e, int enable)
+{
+    if (!e) return set_err("dqmc_kernel_timing: null engine");
+    CU(cudaSetDevice(e->desc.device));
+    CU(cudaStreamSynchronize(e->stream));
+    for (cudaEvent_t v : e->ev) cudaEventDestroy(v);
+    e->ev.clear();
+    e->ev_kind.clear();
+    e->timing = enable != 0;
+    return 0;
+}
+
+int dqmc_kernel_times(dqmc_engine *e, double *sweep_ms, int *sweep_launches,
+                      double *measure_ms, int *measure_launches)
+{
+    if (!e) return set_err("dqmc_kernel_times: null engine");
+    CU(cudaSetDevice(e->desc.device));
+    CU(cudaStreamSynchronize(e->stream));
+    double t[2] = {0.0, 0.0};
+    int c[2] = {0, 0};
+    for (size_t i = 0; i + 1 < e->ev.size(); i += 2) {
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, e->ev[i], e->ev[i + 1]));
+        const int k = e->ev_kind[i];
+        t[k] += ms;
+        c[k] += 1;
+    }
+    if (sweep_ms) *sweep_ms = t[0];
+    if (sweep_launches) *sweep_launches = c[0];
+    if (measure_ms) *measure_ms = t[1];
+    if (measure_launches) *measure_launches = c[1];
+    return 0;
+}
+
+int dqmc_timer_mark(dqmc_engine *e, int which)
+{
+    if (!e || which < 0 || which > 1) return set_err("dqmc_timer_mark: bad arguments");
+    CU(cudaSetDevice(e->desc.device));
+    if (!e->mark[which]) CU(cudaEventCreate(&e->mark[which]));
+    CU(cudaEventRecord(e->mark[which], e->stream));
+    return 0;
+}
+
+int dqmc_timer_elapsed(dqmc_engine *e, double *ms)
+{
+    if (!e || !e->mark[0] || !e->mark[1]) return set_err("dqmc_timer_elapsed: marks missing");
+    CU(cudaEventSynchronize(e->mark[1]));
+    float f = 0.f;
+    CU(cudaEventElapsedTime(&f, e->mark[0], e->mark[1]));
+    *ms = f;
     return 0;
 }
 

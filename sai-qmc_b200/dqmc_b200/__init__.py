@@ -88,6 +88,10 @@ def lib():
                                  C.c_void_p]
     L.dqmc_clear_bins.argtypes = [C.c_void_p]
     L.dqmc_read_profile.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    L.dqmc_kernel_timing.argtypes = [C.c_void_p, C.c_int]
+    L.dqmc_kernel_times.argtypes = [C.c_void_p] + [C.c_void_p] * 4
+    L.dqmc_timer_mark.argtypes = [C.c_void_p, C.c_int]
+    L.dqmc_timer_elapsed.argtypes = [C.c_void_p, C.c_void_p]
     L.dqmc_green_from_scratch.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp,
                                           C.POINTER(C.c_int)]
     L.dqmc_wrap_green.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
@@ -279,6 +283,24 @@ class Engine:
         out = (C.c_ulonglong * len(PHASES))()
         _check(lib().dqmc_read_profile(self.h, c, out, len(PHASES)), "read_profile")
         return dict(zip(PHASES, [int(x) for x in out]))
+
+    def kernel_timing(self, enable=True):
+        _check(lib().dqmc_kernel_timing(self.h, int(enable)), "kernel_timing")
+
+    def kernel_times(self):
+        """(sweep ms, sweep launches, measure ms, measure launches)."""
+        a, b, c, d = C.c_double(), C.c_int(), C.c_double(), C.c_int()
+        _check(lib().dqmc_kernel_times(self.h, C.byref(a), C.byref(b), C.byref(c),
+                                       C.byref(d)), "kernel_times")
+        return a.value, b.value, c.value, d.value
+
+    def mark(self, which):
+        _check(lib().dqmc_timer_mark(self.h, which), "timer_mark")
+
+    def elapsed_ms(self):
+        ms = C.c_double()
+        _check(lib().dqmc_timer_elapsed(self.h, C.byref(ms)), "timer_elapsed")
+        return ms.value
 
     def clear_bins(self):
         _check(lib().dqmc_clear_bins(self.h), "clear_bins")

@@ -33,6 +33,10 @@ CASES = [
     ("sq8_b4", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 2, "af"),
 ]
 
+# the headline lattice: 16x16 U=4 dtau=0.1 beta=8 stab=8, chains seeded as
+# the benchmark's replicas (replica_seed(11, 0, r)); fields and drift only
+HEADLINE = dict(Lx=16, U=4.0, dtau=0.1, L=80, stab=8, base_seed=11, chains=2, sweeps=3)
+
 
 def _read_tokens(path):
     with open(path) as f:
@@ -111,6 +115,28 @@ def main():
             szz=np.array(szz), sperp=np.array(sperp), drift=R.drift(ch),
             rng_end=st["rng"])
         ch.free()
+    h = HEADLINE
+    seeds, fields, drifts, cnts, Gend = [], [], [], [], []
+    for r in range(h["chains"]):
+        seed = R.replica_seed(h["base_seed"], 0, r)
+        ch = R.chain(LAT_SQUARE, h["Lx"], h["Lx"], h["U"], h["dtau"], h["L"], h["stab"], seed,
+                     drift=True)
+        fr = []
+        for _ in range(h["sweeps"]):
+            ch.sweep(1)
+            fr.append(ch.state()["field"])
+        st = ch.state()
+        seeds.append(seed)
+        fields.append(fr)
+        drifts.append(R.drift(ch))
+        cnts.append([st["attempts"], st["accepted"]])
+        Gend.append(st["Gu"][:8, :8])
+        ch.free()
+    np.savez_compressed(os.path.join(HERE, "sq16_b8.npz"),
+                        params=np.array([h["Lx"], h["L"], h["stab"], h["sweeps"]]),
+                        U=h["U"], dtau=h["dtau"], seeds=np.array(seeds, dtype=np.uint64),
+                        fields=np.array(fields), drift=np.array(drifts),
+                        counters=np.array(cnts, dtype=np.int64), G_corner=np.array(Gend))
     udv_fixture(os.path.join(HERE, "udv_fixture.npz"))
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 

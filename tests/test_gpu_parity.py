@@ -166,3 +166,28 @@ def test_u0_exact_free_fermions():
     exact = np.array([np.sum(f * (1 - np.roll(f, -q))) / 8.0 for q in range(4)])
     assert np.max(np.abs(zz[0] - exact)) < 1e-8
     assert np.max(np.abs(pp[0] - 2 * zz[0])) < 1e-12
+
+
+def test_headline_lattice_trajectory_matches_reference():
+    """16x16, U=4, dtau=0.1, beta=8, stab=8 (the benchmark lattice), chains
+    seeded as the benchmark's replicas: the GPU flips exactly the fields the
+    reference flips over the first sweeps, and its reference-definition drift
+    (rebuild from scratch at every stabilization) is of the same size."""
+    g = golden("sq16_b8")
+    Lx, L, stab, sweeps = (int(x) for x in g["params"])
+    T, bp = dq.square_lattice(Lx, Lx)
+    eng = dq.Engine(drift=dq.DRIFT_STAB | dq.DRIFT_SCRATCH)
+    m = eng.add_model(T, bp, float(g["U"]), float(g["dtau"]), Lx, Lx)
+    for s in g["seeds"]:
+        eng.add_chain(m, L, stab, int(s))
+    eng.prepare(1)
+    for s in range(sweeps):
+        eng.sweep(1)
+        for c in range(len(g["seeds"])):
+            diff = int(np.sum(eng.field(c) != g["fields"][c][s]))
+            assert diff == 0, f"chain {c} sweep {s}: {diff} sites differ from the reference"
+    for c in range(len(g["seeds"])):
+        cnt = eng.counters(c)
+        assert (cnt["attempts"], cnt["accepted"]) == tuple(int(x) for x in g["counters"][c])
+        assert cnt["scratch_drift_samples"] == int(g["drift"][c][0])
+        assert cnt["scratch_drift_max"] < 10 * max(g["drift"][c][1], 1e-4)
