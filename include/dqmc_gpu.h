@@ -179,6 +179,21 @@ int dqmc_udv_green(int device, int n, const double *U, const double *D,
  * src/linalg.c:319-346). */
 int dqmc_expm_sym(int n, const double *A, double scale, double *out);
 
+/* No counterpart in the reference.  dqmc_udv_green for callers that must
+ * not allocate device memory (their device memory is owned by their own
+ * allocator, or they cannot afford the device-wide synchronization that
+ * cudaMalloc/cudaFree can cause): the same arguments and result, computed
+ * with a fixed scratch array inside the library instead of allocations.
+ * n is limited to DQMC_NOALLOC_MAX_N; larger n is rejected with an error.
+ * The array (about 1.1 MB) is held by every GPU that loads the library
+ * until exit; the first call on a device also does that device's one-time
+ * set-up, so make it before any stream capture on the device.  All calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialized by the caller. */
+#define DQMC_NOALLOC_MAX_N 128
+int dqmc_udv_green_noalloc(int device, int n, const double *U, const double *D,
+                           const double *T, double *G, int *det_sign);
+
 #ifdef __cplusplus
 }
 #endif

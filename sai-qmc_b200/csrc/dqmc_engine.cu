@@ -127,6 +127,12 @@ struct HChain {
 
 }  // namespace
 
+namespace dqmc_internal {
+/* lets other translation units of the library report through
+ * dqmc_last_error() */
+void set_error(const char *msg) { g_err = msg; }
+}  // namespace dqmc_internal
+
 struct dqmc_engine {
     dqmc_engine_desc desc;
     std::vector<HModel> models;

@@ -98,6 +98,8 @@ def lib():
     L.dqmc_udv_green.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                  C.POINTER(C.c_int)]
     L.dqmc_expm_sym.argtypes = [C.c_int, _dp, C.c_double, _dp]
+    L.dqmc_udv_green_noalloc.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
+                                         C.POINTER(C.c_int)]
     _lib = L
     return L
 
@@ -339,6 +341,18 @@ def udv_green(U, D, T, device=0):
     _check(lib().dqmc_udv_green(device, n, _cm(U),
                                 np.ascontiguousarray(D, dtype=np.float64), _cm(T), g,
                                 C.byref(ds)), "udv_green")
+    return _from_cm(g, n), ds.value
+
+
+def udv_green_noalloc(U, D, T, device=0):
+    """As udv_green, through the entry point that allocates no device
+    memory (fixed in-library scratch, n <= 128; dqmc_udv_green_noalloc)."""
+    n = U.shape[0]
+    g = np.zeros(n * n)
+    ds = C.c_int()
+    _check(lib().dqmc_udv_green_noalloc(device, n, _cm(U),
+                                        np.ascontiguousarray(D, dtype=np.float64), _cm(T),
+                                        g, C.byref(ds)), "udv_green_noalloc")
     return _from_cm(g, n), ds.value
 
 
