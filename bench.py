@@ -224,9 +224,10 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------ GPU arm
-def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB):
+def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB, ctas_per_sm=0):
     T, bp = dq.square_lattice(LX, LX)
-    eng = dq.Engine(device=device, precision=precision, delay_rank=delay_rank)
+    eng = dq.Engine(device=device, precision=precision, delay_rank=delay_rank,
+                    ctas_per_sm=ctas_per_sm)
     m = eng.add_model(T, bp, U, DTAU, LX, LX, szz="af", sperp="af")
     for r in range(chains):
         eng.add_chain(m, L_SLICES, STAB, dq_replica_seed(SEED, 0, seed0 + r))
@@ -304,7 +305,8 @@ def run_gpu_arm(args):
     props = torch.cuda.get_device_properties(local)
     chains = args.chains or 2 * props.multi_processor_count
     precision = dq.PREC_MIXED if args.precision == "mixed" else dq.PREC_FP64
-    eng = make_engine(dq, chains, rank * chains, precision, device=local)
+    eng = make_engine(dq, chains, rank * chains, precision, device=local,
+                      ctas_per_sm=args.ctas_per_sm)
     nbin = max(1, args.steps)
     eng.prepare(nbin)
     for w in range(args.warmup):
@@ -351,11 +353,13 @@ def run_gpu_arm(args):
         flops_launch = chains * flops_per_chain_sweep(N_SITES, L_SLICES, STAB, acc_per_chain_sweep)
         avg_launch = sweep_ms / max(1, nsweep)
         achieved = flops_launch / (avg_launch * 1e-3) / 1e12
-        try:
-            peak = fp64_gemm_peak_tflops()
-            peak_src = "measured: cuBLAS DGEMM 8192^3 on this GPU (bench.py)"
-        except Exception as exc:  # pragma: no cover
-            peak, peak_src = 40.0, f"nominal FP64 (DGEMM probe failed: {exc})"
+        peak, peak_src = 40.0, "nominal B200 FP64 tensor (DGEMM probe skipped)"
+        if not args.no_peak:
+            try:
+                peak = fp64_gemm_peak_tflops()
+                peak_src = "measured: cuBLAS DGEMM 8192^3 on this GPU (bench.py)"
+            except Exception as exc:  # pragma: no cover
+                peak_src = f"nominal B200 FP64 tensor (DGEMM probe failed: {exc})"
         tb = traffic_per_chain_sweep()
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak,
                     "unit": "TFLOP/s", "frac": achieved / peak,
@@ -417,6 +421,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single-chain", action="store_true")
+    ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe")
+    ap.add_argument("--ctas-per-sm", type=int, default=0, choices=[0, 1, 2],
+                    help="sweep kernel residency (0: automatic)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)   # at least three untimed steps
     if args.impl == "reference":
