@@ -94,9 +94,17 @@ using TWide = Tile<16, 128, 16, 1, 8>;  /* 16-row results (V^T X, trsm)    */
  * 32 x 16 = 2 x 2 mma.m16n8k4 fragments; 16 x 128 with 1 x 8 warps. */
 using TMma = Tile<64, 64, 16, 4, 4, true, 2>;
 using TMmaWide = Tile<16, 128, 16, 2, 4, true, 1>;
+/* 128 x 64 with 2 x 4 warps: 4 x 2 fragments per warp, twice the
+ * independent accumulators per warp (needs the full register file) */
+using TMmaBig = Tile<128, 64, 16, 8, 4, true, 2>;
+#if DQMC_MINB == 1
+using TSquare = TMmaBig;
+#else
+using TSquare = TMma;
+#endif
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
-constexpr int GEMM_SMEM =
-    cmax(cmax(TWide::SMEM, TSq::SMEM), cmax(TMma::SMEM, TMmaWide::SMEM));
+constexpr int GEMM_SMEM = cmax(cmax(TWide::SMEM, TSq::SMEM),
+                               cmax(cmax(TMma::SMEM, TMmaWide::SMEM), TSquare::SMEM));
 
 /* D = A(16x4) B(4x8) + C, FP64 on the tensor cores (sm_90+ shape). */
 __device__ __forceinline__ void dmma_16x8x4(double *c, double a0, double a1, double b0)
@@ -311,8 +319,10 @@ __device__ __forceinline__ void gemm_sq(int M, int N, int K, LA la, LB lb, ST st
 {
     if (M <= 32 && N <= 32)
         gemm<TSm, AMF, BKF>(M, N, K, la, lb, st, sm);
-    else
+    else if (M <= 64)
         gemm<TMma, AMF, BKF>(M, N, K, la, lb, st, sm);
+    else
+        gemm<TSquare, AMF, BKF>(M, N, K, la, lb, st, sm);
 }
 
 /* ------------------------------------------------------------ workspace */
@@ -445,7 +455,7 @@ __device__ __noinline__ void apply_block(int m, int nb, const double *P, const d
                 if (i < nb) W[i + j * QNB] = o[i];
         }
         __syncthreads();
-        gemm_rmw<TMma, true, true>(
+        gemm_rmw<TSquare, true, true>(
             m, ncc, nb, [=](int i, int k) { return vpan(P, m, i, k); },
             [=](int k, int j) { return W[k + j * QNB]; },
             [=](int i, int j) { return Xc[i + (size_t)j * ldx]; },
