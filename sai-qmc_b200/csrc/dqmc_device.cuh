@@ -68,10 +68,13 @@ __device__ double block_reduce(double v, double *red)
 /* Tile configuration: BM x BN output tile, BK-deep k slices, each thread
  * owns a TM x TN register tile at rows ty + TY*r, cols tx + TX*c (strided so
  * that shared-memory reads are broadcast or conflict-free). */
-template <int BM_, int BN_, int BK_, int TM_, int TN_, bool MMA_ = false, int WM_ = 2>
+template <int BM_, int BN_, int BK_, int TM_, int TN_, bool MMA_ = false, int WM_ = 2, int KS_ = 4>
 struct Tile {
     static constexpr int BM = BM_, BN = BN_, BK = BK_, TM = TM_, TN = TN_;
     static constexpr bool MMA = MMA_;
+    /* k extent of one mma instruction: m16n8k4, m16n8k8 or m16n8k16 */
+    static constexpr int KS = KS_;
+    static_assert(BK % KS_ == 0, "k slice must hold whole mma steps");
     /* DMMA layout: WM x WN warps, each FM x FN m16n8 fragments */
     static constexpr int WM = WM_, WN = NW / WM_;
     static constexpr int FM = BM / (WM * 16), FN = BN / (WN * 8);
@@ -106,14 +109,33 @@ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int GEMM_SMEM = cmax(cmax(TWide::SMEM, TSq::SMEM),
                                cmax(cmax(TMma::SMEM, TMmaWide::SMEM), TSquare::SMEM));
 
-/* D = A(16x4) B(4x8) + C, FP64 on the tensor cores (sm_90+ shape). */
-__device__ __forceinline__ void dmma_16x8x4(double *c, double a0, double a1, double b0)
+/* D = A(16xKS) B(KSx8) + C, FP64 on the tensor cores.  Fragments: lane
+ * (gid = lane/4, tig = lane%4) holds a[2q] = A(gid, tig+4q), a[2q+1] =
+ * A(gid+8, tig+4q), b[q] = B(tig+4q, gid), c = D(gid|gid+8, 2tig|2tig+1). */
+template <int KS>
+__device__ __forceinline__ void dmma(double *c, const double *a, const double *b)
 {
-    asm volatile(
-        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-        "{%0,%1,%2,%3};\n"
-        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-        : "d"(a0), "d"(a1), "d"(b0));
+    if constexpr (KS == 4) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+            : "d"(a[0]), "d"(a[1]), "d"(b[0]));
+    } else if constexpr (KS == 8) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+            "{%8,%9}, {%0,%1,%2,%3};\n"
+            : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+    } else {
+        static_assert(KS == 16, "mma k extent");
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+            "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+            : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]),
+              "d"(a[7]), "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+    }
 }
 
 /* C(M x N) <- epilogue of sum_k la(i,k) * lb(k,j).
@@ -230,24 +252,28 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
         const double *a = As + cur * BK * AP;
         const double *b = Bs + cur * BK * BP;
         if constexpr (T::MMA) {
-            constexpr int FM = T::FM, FN = T::FN;
+            constexpr int FM = T::FM, FN = T::FN, KS = T::KS, KQ = KS / 4;
 #pragma unroll
-            for (int kk = 0; kk < BK; kk += 4) {
-                double a0[FM], a1[FM], b0[FN];
+            for (int kk = 0; kk < BK; kk += KS) {
+                double af[FM][2 * KQ], bf[FN][KQ];
 #pragma unroll
                 for (int mi = 0; mi < FM; ++mi) {
                     const int i = wm * (FM * 16) + mi * 16 + gid;
-                    a0[mi] = a[(kk + tig) * AP + i];
-                    a1[mi] = a[(kk + tig) * AP + i + 8];
+#pragma unroll
+                    for (int q = 0; q < KQ; ++q) {
+                        af[mi][2 * q] = a[(kk + tig + 4 * q) * AP + i];
+                        af[mi][2 * q + 1] = a[(kk + tig + 4 * q) * AP + i + 8];
+                    }
                 }
 #pragma unroll
                 for (int ni = 0; ni < FN; ++ni)
-                    b0[ni] = b[(kk + tig) * BP + wn * (FN * 8) + ni * 8 + gid];
+#pragma unroll
+                    for (int q = 0; q < KQ; ++q)
+                        bf[ni][q] = b[(kk + tig + 4 * q) * BP + wn * (FN * 8) + ni * 8 + gid];
 #pragma unroll
                 for (int mi = 0; mi < FM; ++mi)
 #pragma unroll
-                    for (int ni = 0; ni < FN; ++ni)
-                        dmma_16x8x4(acc[mi * FN + ni], a0[mi], a1[mi], b0[ni]);
+                    for (int ni = 0; ni < FN; ++ni) dmma<KS>(acc[mi * FN + ni], af[mi], bf[ni]);
             }
         } else {
 #pragma unroll
@@ -326,57 +352,126 @@ __device__ __forceinline__ void gemm_sq(int M, int N, int K, LA la, LB lb, ST st
 }
 
 /* ------------------------------------------------------------ workspace */
-/* Shared-memory carve-up of one CTA (sizes in doubles, all disjoint
- * except the phase union, which the QR and the site-block update share). */
+/* Shared-memory resident QR (qr_*_sm): the active block of cb columns (or,
+ * transposed, rows) lives in shared memory with leading dimension
+ * qr_ld(n) = round16(n) + 4 (so DMMA fragment reads hit distinct banks),
+ * next to one reflector panel V (qr_ld x 16), the panel product W and
+ * small scratch.  cb is the widest of 64/48/32/16 that fits the CTA's
+ * shared-memory budget; 0 selects the global-memory QR. */
+constexpr int QW = 20;              /* leading dimension of W (16 rows) */
+constexpr size_t QR_MISC = 1920;    /* T, gram, taus, reductions        */
+constexpr size_t SMEM_BUDGET = (DQMC_MINB == 1 ? 227 * 1024 : 113 * 1024) / 8;
+
+__host__ __device__ inline int qr_ld(int n) { return ((n + 15) / 16) * 16 + 4; }
+__host__ __device__ inline size_t qr_wp(int cb)
+{
+    const size_t a = (size_t)NW * 128, b = (size_t)QW * cb;
+    return a > b ? a : b;
+}
+__host__ __device__ inline size_t qr_sm_doubles(int n, int cb)
+{
+    return (size_t)qr_ld(n) * (cb + 16) + (size_t)QW * cb + qr_wp(cb) + QR_MISC;
+}
+__host__ __device__ inline size_t smem_fixed(int n)
+{
+    const size_t ints = (size_t)n + 2 * DQMC_MAX_KB + 8;
+    return ((40 + 4 * (size_t)n + (ints + 1) / 2) + 1) & ~(size_t)1;
+}
+__host__ __device__ inline size_t smem_gemm_union(int n)
+{
+    const size_t qr = (size_t)n * QNB + (size_t)QNB * WCOLS + 2 * QNB * QNB + QNB;
+    const size_t pr = 4 * (size_t)DQMC_MAX_KB * (DQMC_MAX_KB + 1) + DQMC_MAX_KB;
+    return (size_t)GEMM_SMEM + (qr > pr ? qr : pr);
+}
+__host__ __device__ inline int qr_cb(int n)
+{
+    if (n > 3 * NT) return 0;
+    const size_t base = smem_fixed(n) + 8;
+    const size_t gu = smem_gemm_union(n);
+    for (int cb = 64; cb >= 16; cb -= 16) {
+        const size_t q = qr_sm_doubles(n, cb);
+        if (base + (q > gu ? q : gu) <= SMEM_BUDGET) return cb;
+    }
+    return 0;
+}
+
+/* Shared-memory carve-up of one CTA (sizes in doubles).  The fixed part
+ * (reductions, per-row vectors, permutation) is followed by a union of
+ * two views: GEMM staging + QR panel / site-block area, or the
+ * shared-memory QR area. */
+struct QrSm {
+    double *X;       /* ld x cb active block                          */
+    double *V;       /* ld x 16 reflector panel, unit diagonal        */
+    double *W;       /* 16 x cb (ld QW) panel product                 */
+    double *Wp;      /* NW x 128 partial products                     */
+    double *T;       /* 16 x 16 compact-WY factor                     */
+    double *gram;    /* 16 x 16 V^T V of the panel                    */
+    double *taus;    /* 16                                            */
+    double *rp;      /* 16 x NW + NW + 8 reduction partials           */
+    double *rf;      /* 16 reduction results                          */
+    int ld, cb;
+};
+
 struct Smem {
     double *gsm;     /* GEMM staging                                 */
     double *red;     /* 40: reductions                               */
     double *vA, *vB, *vC, *vD;  /* n each: scalings, new log D, signs, norms */
     int *perm;       /* n                                            */
     int *iscr;       /* 2*DQMC_MAX_KB + 8 ints                       */
-    double *phase;   /* union area                                   */
-    /* QR view of the union area */
+    double *phase;   /* area after the GEMM staging                  */
+    /* global-memory QR view of the phase area */
     double *P, *W, *Tw, *gram, *taus;
-    /* site-block view of the union area */
+    /* site-block view of the phase area */
     double *g0, *gt, *gam, *xs, *colA;
+    QrSm q;          /* shared-memory QR view (overlaps gsm + phase) */
 };
 
 __host__ __device__ inline size_t smem_doubles(int n, int kb)
 {
-    const size_t qr = (size_t)n * QNB + (size_t)QNB * WCOLS + 2 * QNB * QNB + QNB;
     (void)kb;
-    const size_t pr = 4 * (size_t)DQMC_MAX_KB * (DQMC_MAX_KB + 1) + DQMC_MAX_KB;
-    const size_t un = qr > pr ? qr : pr;
-    const size_t ints = (size_t)n + 2 * DQMC_MAX_KB + 8;
-    return (size_t)GEMM_SMEM + 40 + 4 * (size_t)n + (ints + 1) / 2 + un + 8;
+    const int cb = qr_cb(n);
+    const size_t gu = smem_gemm_union(n);
+    const size_t q = cb ? qr_sm_doubles(n, cb) : 0;
+    return smem_fixed(n) + (q > gu ? q : gu) + 8;
 }
 
 __device__ inline Smem carve(double *base, int n, int kb)
 {
     Smem s;
     double *p = base;
-    s.gsm = p; p += GEMM_SMEM;
     s.red = p; p += 40;
     s.vA = p; p += n;
     s.vB = p; p += n;
     s.vC = p; p += n;
     s.vD = p; p += n;
-    const size_t ints = (size_t)n + 2 * DQMC_MAX_KB + 8;
     s.perm = (int *)p;
     s.iscr = s.perm + n;
-    p += (ints + 1) / 2;
-    s.phase = p;
-    s.P = p;
+    p = base + smem_fixed(n);
+    s.gsm = p;
+    s.phase = p + GEMM_SMEM;
+    s.P = s.phase;
     s.W = s.P + (size_t)n * QNB;
     s.Tw = s.W + (size_t)QNB * WCOLS;
     s.gram = s.Tw + QNB * QNB;
     s.taus = s.gram + QNB * QNB;
     const int ld = kb + 1;
-    s.g0 = p;
+    s.g0 = s.phase;
     s.gt = s.g0 + (size_t)kb * ld;
     s.gam = s.gt + (size_t)kb * ld;
     s.xs = s.gam + (size_t)kb * ld;
     s.colA = s.xs + kb;
+    QrSm &q = s.q;
+    q.ld = qr_ld(n);
+    q.cb = qr_cb(n);
+    q.X = p;
+    q.V = q.X + (size_t)q.ld * q.cb;
+    q.W = q.V + (size_t)q.ld * 16;
+    q.Wp = q.W + (size_t)QW * q.cb;
+    q.T = q.Wp + qr_wp(q.cb);
+    q.gram = q.T + 256;
+    q.taus = q.gram + 256;
+    q.rp = q.taus + 16;
+    q.rf = q.rp + 16 * NW + NW + 8;
     return s;
 }
 
@@ -467,7 +562,7 @@ __device__ __noinline__ void apply_block(int m, int nb, const double *P, const d
  * layout and dlarfg sign convention.  tw receives each panel's Tw
  * (QNB*QNB per panel).  Returns the number of non-trivial reflectors (the
  * parity gives det Q). */
-__device__ __noinline__ int qr_factor(int n, double *A, double *tw, Smem &s, int *flag)
+__device__ __noinline__ int qr_factor_gm(int n, double *A, double *tw, Smem &s, int *flag)
 {
     int nontrivial = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -544,7 +639,8 @@ __device__ __noinline__ void load_panel(int n, const double *A, const double *tw
 }
 
 /* Q = H_1 ... H_n of a factored A written to Q (ld n). */
-__device__ __noinline__ void qr_form_q(int n, const double *A, const double *tw, double *Q, Smem &s)
+__device__ __noinline__ void qr_form_q_gm(int n, const double *A, const double *tw, double *Q,
+                                          Smem &s)
 {
     for (int e = threadIdx.x; e < n * n; e += NT) Q[e] = (e % n == e / n) ? 1.0 : 0.0;
     __syncthreads();
@@ -556,8 +652,8 @@ __device__ __noinline__ void qr_form_q(int n, const double *A, const double *tw,
 }
 
 /* Y (n x nc, ld n) <- Q^T Y for a factored A. */
-__device__ __noinline__ void qr_apply_qt(int n, const double *A, const double *tw, double *Y, int nc,
-                            Smem &s)
+__device__ __noinline__ void qr_apply_qt_gm(int n, const double *A, const double *tw, double *Y,
+                                            int nc, Smem &s)
 {
     for (int j0 = 0; j0 < n; j0 += QNB) {
         load_panel(n, A, tw, j0, s);
@@ -678,6 +774,530 @@ __device__ int qr_diag(int n, const double *A, Smem &s, int *flag)
     return (((long long)neg) & 1) ? -1 : 1;
 }
 
+/* ------------------------------------------- shared-memory resident QR */
+/* The factorization of qr_factor_gm (dgeqrf layout in A, dlarfg signs,
+ * forward columnwise compact-WY factors in tw, so either routine's output
+ * feeds the other's form/apply routines), organised so that one CTA works
+ * out of shared memory:
+ *  - left-looking over blocks of cb columns: a block is loaded once, the
+ *    earlier panels' block reflectors are applied to it from a staged
+ *    panel V, its own panels are factored in place and it is stored once;
+ *  - a panel is factored with its rows in registers (panel row r on thread
+ *    r mod NT): per column one CTA reduction for the norm and one 16-wide
+ *    reduction for the dot products with the trailing panel columns; the
+ *    compact-WY factor (dlarft) comes from V^T V on the tensor cores;
+ *  - W = V^T X, op(T) W and X -= V W run on the FP64 tensor cores with
+ *    every operand in shared memory.
+ * Padding rows (to round16(n)) of the block and of V are kept at zero so
+ * the 16-deep mma steps may run past the matrix edge. */
+
+/* v[c] <- CTA-wide sum of v[c], c < 16, in every thread. */
+__device__ __forceinline__ void block_sum16(double (&v)[16], double *rp, double *rf)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+    double h8[8], h4[4], h2[2];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const double send = b4 ? v[k] : v[k + 8], keep = b4 ? v[k + 8] : v[k];
+        h8[k] = keep + __shfl_xor_sync(FULL, send, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double send = b3 ? h8[k] : h8[k + 4], keep = b3 ? h8[k + 4] : h8[k];
+        h4[k] = keep + __shfl_xor_sync(FULL, send, 8);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double send = b2 ? h4[k] : h4[k + 2], keep = b2 ? h4[k + 2] : h4[k];
+        h2[k] = keep + __shfl_xor_sync(FULL, send, 4);
+    }
+    double h1;
+    {
+        const double send = b1 ? h2[0] : h2[1], keep = b1 ? h2[1] : h2[0];
+        h1 = keep + __shfl_xor_sync(FULL, send, 2);
+    }
+    h1 += __shfl_xor_sync(FULL, h1, 1);
+    /* the warp sum of value (lane >> 1) & 15 */
+    if ((lane & 1) == 0) rp[((lane >> 1) & 15) * NW + warp] = h1;
+    __syncthreads();
+    if (threadIdx.x < 16) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) t += rp[threadIdx.x * NW + w];
+        rf[threadIdx.x] = t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; ++c) v[c] = rf[c];
+}
+
+/* Partial products of V^T Xr (16 x nc, K = m rows): warp (f, g) computes
+ * column fragment f over the g-th share of the 16-deep k steps. */
+__device__ void qr_vtx(QrSm &q, const double *Xr, int m, int nc)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int ld = q.ld;
+    const int nfr = (nc + 7) >> 3, ngr = NW / nfr, nks = (m + 15) >> 4;
+    if (warp < nfr * ngr) {
+        const int f = warp % nfr, g = warp / nfr;
+        const int ks0 = g * nks / ngr, ks1 = (g + 1) * nks / ngr;
+        const double *vb = q.V + tig + (size_t)gid * ld;
+        const double *xb = Xr + tig + (size_t)(f * 8 + gid) * ld;
+        double c0[4] = {0.0, 0.0, 0.0, 0.0}, c1[4] = {0.0, 0.0, 0.0, 0.0};
+        int ks = ks0;
+        for (; ks + 1 < ks1; ks += 2) {
+            double a0[8], b0[4], a1[8], b1[4];
+            const int k0 = ks * 16, k1 = k0 + 16;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a0[2 * u] = vb[k0 + 4 * u];
+                a0[2 * u + 1] = vb[k0 + 4 * u + 8 * ld];
+                b0[u] = xb[k0 + 4 * u];
+                a1[2 * u] = vb[k1 + 4 * u];
+                a1[2 * u + 1] = vb[k1 + 4 * u + 8 * ld];
+                b1[u] = xb[k1 + 4 * u];
+            }
+            dmma<16>(c0, a0, b0);
+            dmma<16>(c1, a1, b1);
+        }
+        if (ks < ks1) {
+            double a0[8], b0[4];
+            const int k0 = ks * 16;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a0[2 * u] = vb[k0 + 4 * u];
+                a0[2 * u + 1] = vb[k0 + 4 * u + 8 * ld];
+                b0[u] = xb[k0 + 4 * u];
+            }
+            dmma<16>(c0, a0, b0);
+        }
+        double *o = q.Wp + (size_t)(g * nfr + f) * 128;
+        o[gid * 8 + 2 * tig] = c0[0] + c1[0];
+        o[gid * 8 + 2 * tig + 1] = c0[1] + c1[1];
+        o[(gid + 8) * 8 + 2 * tig] = c0[2] + c1[2];
+        o[(gid + 8) * 8 + 2 * tig + 1] = c0[3] + c1[3];
+    }
+    __syncthreads();
+}
+
+/* q.V <- reflectors (unit diagonal, zero above and in the padding) of the
+ * panel whose tails are at src (ld lds, m rows, nb columns). */
+__device__ __forceinline__ void qr_stage_v(QrSm &q, const double *src, size_t lds, int m, int nb)
+{
+    const int R = (m + 15) & ~15, ld = q.ld;
+    for (int r = threadIdx.x; r < R; r += NT) {
+        double v[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            v[c] = (c < nb && r < m && r > c) ? src[r + c * lds] : 0.0;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) q.V[r + c * ld] = (r == c && c < nb) ? 1.0 : v[c];
+    }
+}
+
+/* Householder panel of nb <= 16 columns, m rows, at Xp (ld q.ld) in
+ * place: R on and above the diagonal, reflector tails below; q.taus, the
+ * staged panel q.V and its compact-WY factor q.T.  Returns the number of
+ * non-trivial reflectors.  The panel's columns jj.. of row r live in
+ * registers x[t][0..] of thread r mod NT (t = r / NT < RPT) and shift
+ * down one slot per column, so the column loop stays rolled. */
+template <int RPT>
+__device__ __noinline__ int qr_panel(QrSm &q, double *Xp, int m, int nb, int *flag)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ld = q.ld;
+    double x[RPT][16];
+#pragma unroll
+    for (int t = 0; t < RPT; ++t) {
+        const int r = tid + NT * t;
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            x[t][c] = (r < m && c < nb) ? Xp[r + (size_t)c * ld] : 0.0;
+    }
+    int nontrivial = 0;
+#pragma unroll 1
+    for (int jj = 0; jj < nb; ++jj) {
+        double sq = 0.0;
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            const int r = tid + NT * t;
+            if (r > jj && r < m) sq = fma(x[t][0], x[t][0], sq);
+        }
+        sq = warp_sum(sq);
+        if (lane == 0) q.rp[16 * NW + warp] = sq;
+        if (tid == jj) q.rp[17 * NW] = x[0][0];
+        __syncthreads();
+        double xn2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) xn2 += q.rp[16 * NW + w];
+        const double alpha = q.rp[17 * NW];
+        double tau = 0.0, beta = alpha, scal = 0.0;
+        if (xn2 > 0.0) {
+            beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+            tau = (beta - alpha) / beta;
+            scal = 1.0 / (alpha - beta);
+            ++nontrivial;
+        }
+        if (tid == 0 && (!isfinite(beta) || !isfinite(tau))) raise_flag(flag, DQMC_ST_NONFINITE);
+        double vr[RPT];
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            const int r = tid + NT * t;
+            const bool below = r > jj && r < m;
+            if (below && xn2 > 0.0) x[t][0] *= scal;
+            vr[t] = (r == jj) ? 1.0 : (below ? x[t][0] : 0.0);
+        }
+        /* d[c] = v^T (panel column jj + c), c >= 1 */
+        double d[16];
+        d[0] = 0.0;
+#pragma unroll
+        for (int c = 1; c < 16; ++c) {
+            double acc = 0.0;
+#pragma unroll
+            for (int t = 0; t < RPT; ++t) acc = fma(vr[t], x[t][c], acc);
+            d[c] = acc;
+        }
+        block_sum16(d, q.rp, q.rf);
+        if (tid == 0) q.taus[jj] = tau;
+        if (tau != 0.0) {
+#pragma unroll
+            for (int c = 1; c < 16; ++c) {
+                const double wc = tau * d[c];
+#pragma unroll
+                for (int t = 0; t < RPT; ++t) x[t][c] = fma(-wc, vr[t], x[t][c]);
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < RPT; ++t) {
+            const int r = tid + NT * t;
+            if (r < m) Xp[r + (size_t)jj * ld] = (r == jj) ? beta : x[t][0];
+#pragma unroll
+            for (int c = 0; c < 15; ++c) x[t][c] = x[t][c + 1];
+            x[t][15] = 0.0;
+        }
+    }
+    __syncthreads();
+    /* gram = V^T V on the tensor cores, then dlarft (forward columnwise):
+     * T[:i, i] = -tau_i T[:i, :i] V^T v_i, T[i, i] = tau_i */
+    qr_stage_v(q, Xp, ld, m, nb);
+    __syncthreads();
+    qr_vtx(q, q.V, m, 16);
+    if (warp == 0) {
+        for (int e = lane; e < 256; e += 32) {
+            const int k = e & 15, i = e >> 4;
+            double g = 0.0;
+            if (k < i) {
+#pragma unroll
+                for (int gg = 0; gg < NW / 2; ++gg)
+                    g += q.Wp[(size_t)(gg * 2 + (i >> 3)) * 128 + k * 8 + (i & 7)];
+            }
+            q.gram[k + i * 16] = g;
+            q.T[e] = 0.0;
+        }
+        __syncwarp();
+        for (int i = 0; i < nb; ++i) {
+            const double ti = q.taus[i];
+            if (lane < i) {
+                double acc = 0.0;
+                for (int k = lane; k < i; ++k) acc += q.T[lane + k * 16] * q.gram[k + i * 16];
+                q.T[lane + i * 16] = -ti * acc;
+            } else if (lane == i) {
+                q.T[i + i * 16] = ti;
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    return nontrivial;
+}
+
+/* q.V <- reflectors of panel p0 of a factored A, q.T <- its factor. */
+__device__ void qr_load_v(QrSm &q, int n, const double *A, const double *tw, int p0)
+{
+    qr_stage_v(q, A + p0 + (size_t)p0 * n, (size_t)n, n - p0, min(16, n - p0));
+    const double *twp = tw + (size_t)(p0 / 16) * 256;
+    for (int e = threadIdx.x; e < 256; e += NT) q.T[e] = twp[e];
+    __syncthreads();
+}
+
+/* q.W (16 x nc, ld QW) <- op(T) * (sum of the partials): T^T for H^T
+ * (trans), T for H; one m16n8k16 per column fragment. */
+__device__ void qr_tw(QrSm &q, int nc, bool trans)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int nfr = (nc + 7) >> 3, ngr = NW / nfr;
+    if (warp < nfr) {
+        const int f = warp;
+        double a[8], b[4], c[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = tig + 4 * u;
+            a[2 * u] = trans ? q.T[k + gid * 16] : q.T[gid + k * 16];
+            a[2 * u + 1] = trans ? q.T[k + (gid + 8) * 16] : q.T[gid + 8 + k * 16];
+            double t = 0.0;
+            for (int g = 0; g < ngr; ++g) t += q.Wp[(size_t)(g * nfr + f) * 128 + k * 8 + gid];
+            b[u] = t;
+        }
+        dmma<16>(c, a, b);
+        double *o = q.W + (f * 8 + 2 * tig) * QW + gid;
+        o[0] = c[0];
+        o[QW] = c[1];
+        o[8] = c[2];
+        o[QW + 8] = c[3];
+    }
+    __syncthreads();
+}
+
+/* Xr (m rows, nc columns) -= V q.W. */
+__device__ void qr_vupd(QrSm &q, double *Xr, int m, int nc)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gid = lane >> 2, tig = lane & 3;
+    const int ld = q.ld;
+    const int nrb = (m + 15) >> 4, nfr = (nc + 7) >> 3;
+    for (int rb = warp; rb < nrb; rb += NW) {
+        const double *vb = q.V + rb * 16 + gid + (size_t)tig * ld;
+        double a[8];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[2 * u] = -vb[(size_t)4 * u * ld];
+            a[2 * u + 1] = -vb[(size_t)4 * u * ld + 8];
+        }
+        double *xb = Xr + rb * 16 + gid;
+#pragma unroll
+        for (int f = 0; f < 8; ++f) {
+            if (f < nfr) {
+                const double *wb = q.W + tig + (f * 8 + gid) * QW;
+                double b[4], c[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) b[u] = wb[4 * u];
+                double *x0 = xb + (size_t)(f * 8 + 2 * tig) * ld;
+                c[0] = x0[0];
+                c[1] = x0[ld];
+                c[2] = x0[8];
+                c[3] = x0[ld + 8];
+                dmma<16>(c, a, b);
+                x0[0] = c[0];
+                x0[ld] = c[1];
+                x0[8] = c[2];
+                x0[ld + 8] = c[3];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+/* Xr <- op(H) Xr for the block reflector staged in q.V / q.T. */
+__device__ __forceinline__ void qr_apply_sm(QrSm &q, double *Xr, int m, int nc, bool trans)
+{
+    qr_vtx(q, Xr, m, nc);
+    qr_tw(q, nc, trans);
+    qr_vupd(q, Xr, m, nc);
+}
+
+/* q.X <- columns [c0, c0+nc) of M (n x *, ld n), zero padding up to
+ * round16(n) rows and cb columns; eight loads in flight per thread. */
+__device__ void qr_load_cols(QrSm &q, int n, const double *M, int c0, int nc)
+{
+    const int R = (n + 15) & ~15, ld = q.ld;
+    for (int cc = 0; cc < q.cb; cc += 8) {
+        for (int r = threadIdx.x; r < R; r += NT) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                v[u] = (r < n && cc + u < nc) ? M[r + (size_t)(c0 + cc + u) * n] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) q.X[r + (size_t)(cc + u) * ld] = v[u];
+        }
+    }
+    __syncthreads();
+}
+
+__device__ void qr_store_cols(QrSm &q, int n, double *M, int c0, int nc)
+{
+    const int ld = q.ld;
+    for (int cc = 0; cc < nc; cc += 8) {
+        for (int r = threadIdx.x; r < n; r += NT) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = q.X[r + (size_t)(cc + u) * ld];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (cc + u < nc) M[r + (size_t)(c0 + cc + u) * n] = v[u];
+        }
+    }
+    __syncthreads();
+}
+
+/* Transposed block: q.X[c + rr*ld] <-> M[(r0 + rr) + c*n] for rr < nr
+ * rows of M and c < n.  A warp covers 8 rows x 4 columns of M per step
+ * (64-byte row runs in global memory, at most two-way bank conflicts). */
+struct QrTmap {
+    int rr, c, cstep;
+    bool active;
+};
+__device__ __forceinline__ QrTmap qr_tmap(int cb)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rg = cb >> 3, ncw = NW / rg;
+    return QrTmap{(lane & 7) + 8 * (warp % rg), (lane >> 3) + 4 * (warp / rg), 4 * ncw,
+                  warp < rg * ncw};
+}
+
+__device__ void qr_load_rows_t(QrSm &q, int n, const double *M, int r0, int nr)
+{
+    const int R = (n + 15) & ~15, ld = q.ld;
+    const QrTmap t = qr_tmap(q.cb);
+    const bool rok = t.rr < nr;
+    const double *src = M + r0 + t.rr;
+    double *dst = q.X + (size_t)t.rr * ld;
+    for (int c0 = t.active ? t.c : R; c0 < R; c0 += 8 * t.cstep) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int c = c0 + u * t.cstep;
+            v[u] = (rok && c < n) ? src[(size_t)c * n] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int c = c0 + u * t.cstep;
+            if (c < R) dst[c] = v[u];
+        }
+    }
+    __syncthreads();
+}
+
+__device__ void qr_store_rows_t(QrSm &q, int n, double *M, int r0, int nr, const double *cs)
+{
+    const int ld = q.ld;
+    const QrTmap t = qr_tmap(q.cb);
+    if (t.active && t.rr < nr) {
+        double *dst = M + r0 + t.rr;
+        const double *src = q.X + (size_t)t.rr * ld;
+        for (int c0 = t.c; c0 < n; c0 += 8 * t.cstep) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int c = c0 + u * t.cstep;
+                v[u] = c < n ? src[c] * cs[c] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int c = c0 + u * t.cstep;
+                if (c < n) dst[(size_t)c * n] = v[u];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __noinline__ int qr_factor_sm(int n, double *A, double *tw, Smem &s, int *flag)
+{
+    QrSm &q = s.q;
+    const int ld = q.ld, cb = q.cb;
+    int nontrivial = 0;
+    for (int jb = 0; jb < n; jb += cb) {
+        const int nc = min(cb, n - jb);
+        qr_load_cols(q, n, A, jb, nc);
+        for (int p0 = 0; p0 < jb; p0 += 16) {
+            qr_load_v(q, n, A, tw, p0);
+            qr_apply_sm(q, q.X + p0, n - p0, nc, true);
+        }
+        for (int pc = 0; pc < nc; pc += 16) {
+            const int j0 = jb + pc, m = n - j0, nb = min(16, m);
+            double *Xp = q.X + j0 + (size_t)pc * ld;
+            if (m <= NT)
+                nontrivial += qr_panel<1>(q, Xp, m, nb, flag);
+            else if (m <= 2 * NT)
+                nontrivial += qr_panel<2>(q, Xp, m, nb, flag);
+            else
+                nontrivial += qr_panel<3>(q, Xp, m, nb, flag);
+            double *twp = tw + (size_t)(j0 / 16) * 256;
+            for (int e = threadIdx.x; e < 256; e += NT) twp[e] = q.T[e];
+            if (pc + 16 < nc) qr_apply_sm(q, Xp + (size_t)16 * ld, m, nc - pc - 16, true);
+        }
+        qr_store_cols(q, n, A, jb, nc);
+    }
+    return nontrivial;
+}
+
+/* Q = H_1 ... H_n (n x n, ld n), column block by column block; panels
+ * that start below a block's last column leave it unchanged. */
+__device__ __noinline__ void qr_form_q_sm(int n, const double *A, const double *tw, double *Q,
+                                          Smem &s)
+{
+    QrSm &q = s.q;
+    const int ld = q.ld, cb = q.cb, R = (n + 15) & ~15;
+    for (int jb = 0; jb < n; jb += cb) {
+        const int nc = min(cb, n - jb);
+        for (int c = 0; c < cb; ++c)
+            for (int r = threadIdx.x; r < R; r += NT)
+                q.X[r + (size_t)c * ld] = (c < nc && r == jb + c) ? 1.0 : 0.0;
+        __syncthreads();
+        for (int p0 = ((jb + nc - 1) / 16) * 16; p0 >= 0; p0 -= 16) {
+            qr_load_v(q, n, A, tw, p0);
+            qr_apply_sm(q, q.X + p0, n - p0, nc, false);
+        }
+        qr_store_cols(q, n, Q, jb, nc);
+    }
+}
+
+/* Y (n x ncols, ld n) <- Q^T Y. */
+__device__ __noinline__ void qr_apply_qt_sm(int n, const double *A, const double *tw, double *Y,
+                                            int ncols, Smem &s)
+{
+    QrSm &q = s.q;
+    for (int jb = 0; jb < ncols; jb += q.cb) {
+        const int nc = min(q.cb, ncols - jb);
+        qr_load_cols(q, n, Y, jb, nc);
+        for (int p0 = 0; p0 < n; p0 += 16) {
+            qr_load_v(q, n, A, tw, p0);
+            qr_apply_sm(q, q.X + p0, n - p0, nc, true);
+        }
+        qr_store_cols(q, n, Y, jb, nc);
+    }
+}
+
+/* Xout = Xin Q diag(cs) (n x n, ld n; Xout may be Xin), a block of rows
+ * at a time as (Xin Q)^T = Q^T Xin^T. */
+__device__ __noinline__ void qr_apply_right_sm(int n, const double *A, const double *tw,
+                                               const double *Xin, double *Xout,
+                                               const double *cs, Smem &s)
+{
+    QrSm &q = s.q;
+    for (int r0 = 0; r0 < n; r0 += q.cb) {
+        const int nr = min(q.cb, n - r0);
+        qr_load_rows_t(q, n, Xin, r0, nr);
+        for (int p0 = 0; p0 < n; p0 += 16) {
+            qr_load_v(q, n, A, tw, p0);
+            qr_apply_sm(q, q.X + p0, n - p0, nr, true);
+        }
+        qr_store_rows_t(q, n, Xout, r0, nr, cs);
+    }
+}
+
+/* Dispatch: shared-memory QR when the block fits, else the global one. */
+__device__ __forceinline__ int qr_factor(int n, double *A, double *tw, Smem &s, int *flag)
+{
+    return s.q.cb ? qr_factor_sm(n, A, tw, s, flag) : qr_factor_gm(n, A, tw, s, flag);
+}
+__device__ __forceinline__ void qr_form_q(int n, const double *A, const double *tw, double *Q,
+                                          Smem &s)
+{
+    if (s.q.cb)
+        qr_form_q_sm(n, A, tw, Q, s);
+    else
+        qr_form_q_gm(n, A, tw, Q, s);
+}
+__device__ __forceinline__ void qr_apply_qt(int n, const double *A, const double *tw, double *Y,
+                                            int nc, Smem &s)
+{
+    if (s.q.cb)
+        qr_apply_qt_sm(n, A, tw, Y, nc, s);
+    else
+        qr_apply_qt_gm(n, A, tw, Y, nc, s);
+}
+
 /* ------------------------------------------------------------------ UDV */
 struct Udv {
     double *U, *T, *ell, *det;
@@ -784,16 +1404,21 @@ __device__ __noinline__ void udv_rmul(int n, Udv u, const double *B, Scr w, Smem
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
     const int sg = qr_diag(n, w.m1, s, flag);
-    qr_form_q(n, w.m1, w.tw, w.m0, s);
-    const double *U = u.U;
-    const double *Q = w.m0;
-    const double *sgn = s.vC;
-    double *Un = w.m2;
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return U[i + (size_t)k * n]; },
-        [=](int k, int j) { return Q[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { Un[i + (size_t)j * n] = v * sgn[j]; }, s.gsm);
-    for (int e = threadIdx.x; e < n * n; e += NT) u.U[e] = Un[e];
+    if (s.q.cb) {
+        /* U <- U Q diag(sign R_ii), Q applied from the right in blocks */
+        qr_apply_right_sm(n, w.m1, w.tw, u.U, u.U, s.vC, s);
+    } else {
+        qr_form_q(n, w.m1, w.tw, w.m0, s);
+        const double *U = u.U;
+        const double *Q = w.m0;
+        const double *sgn = s.vC;
+        double *Un = w.m2;
+        gemm_sq<true, true>(
+            n, n, n, [=](int i, int k) { return U[i + (size_t)k * n]; },
+            [=](int k, int j) { return Q[k + (size_t)j * n]; },
+            [=](int i, int j, double v) { Un[i + (size_t)j * n] = v * sgn[j]; }, s.gsm);
+        for (int e = threadIdx.x; e < n * n; e += NT) u.U[e] = Un[e];
+    }
     const double *R = w.m1;
     for (int e = threadIdx.x; e < n * n; e += NT) {
         const int i = e % n, r = e / n;
@@ -828,13 +1453,17 @@ __device__ __noinline__ void udv_combine(int n, Udv l, Udv r, Udv o, Scr w, Smem
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
     const int sg = qr_diag(n, w.m1, s, flag);
-    qr_form_q(n, w.m1, w.tw, w.m0, s);
-    const double *UL = l.U, *Q = w.m0, *sgn = s.vC;
-    double *Uo = o.U;
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return UL[i + (size_t)k * n]; },
-        [=](int k, int j) { return Q[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { Uo[i + (size_t)j * n] = v * sgn[j]; }, s.gsm);
+    if (s.q.cb) {
+        qr_apply_right_sm(n, w.m1, w.tw, l.U, o.U, s.vC, s);
+    } else {
+        qr_form_q(n, w.m1, w.tw, w.m0, s);
+        const double *UL = l.U, *Q = w.m0, *sgn = s.vC;
+        double *Uo = o.U;
+        gemm_sq<true, true>(
+            n, n, n, [=](int i, int k) { return UL[i + (size_t)k * n]; },
+            [=](int k, int j) { return Q[k + (size_t)j * n]; },
+            [=](int i, int j, double v) { Uo[i + (size_t)j * n] = v * sgn[j]; }, s.gsm);
+    }
     const double *R = w.m1, *TR = r.T;
     const int *perm = s.perm;
     double *To = o.T;
