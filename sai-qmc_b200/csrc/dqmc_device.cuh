@@ -9,6 +9,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "dqmc_common.h"
 
 /* The device code is compiled twice (dqmc_k1.cu, dqmc_k2.cu) into distinct
@@ -149,8 +151,15 @@ __device__ __forceinline__ void dmma(double *c, const double *a, const double *b
  * slice -- possibly of the next output tile -- is fetched into registers
  * while the current one is multiplied, so short-K products stay busy.
  * Every thread of the CTA must call this. */
-template <class T, bool AMF, bool BKF, bool RMW, class LA, class LB, class LC, class ST>
-__device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, double *sm)
+/* Operand transform applied when a fetched slice is staged (identity). */
+struct Ident {
+    __device__ __forceinline__ double operator()(int, int, double x) const { return x; }
+};
+
+template <class T, bool AMF, bool BKF, bool RMW, class LA, class LB, class LC, class ST,
+          class SA = Ident, class SB = Ident>
+__device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, double *sm,
+                          SA sa = SA(), SB sb = SB())
 {
     constexpr int BM = T::BM, BN = T::BN, BK = T::BK, TM = T::TM, TN = T::TN;
     constexpr int TX = T::TX, TY = T::TY, AP = T::AP, BP = T::BP;
@@ -208,18 +217,30 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
             rb[q] = (gk < K && gj < N) ? lb(gk, gj) : 0.0;
         }
     };
+    /* Loaders only load: any arithmetic on a loaded value (sa, sb) runs
+     * here, after the slice's math, so the loads stay in flight across it. */
     auto put = [&](int buf) {
 #pragma unroll
         for (int q = 0; q < AL; ++q) {
             const int e = tid + q * NT;
             const int i = AMF ? e % BM : e / BK, k = AMF ? e / BM : e % BK;
-            As[buf * BK * AP + k * AP + i] = ra[q];
+            double v = ra[q];
+            if constexpr (!std::is_same<SA, Ident>::value) {
+                const int gi = fm0 + i, gk = fk0 + k;
+                v = (gi < M && gk < K) ? sa(gi, gk, v) : 0.0;
+            }
+            As[buf * BK * AP + k * AP + i] = v;
         }
 #pragma unroll
         for (int q = 0; q < BL; ++q) {
             const int e = tid + q * NT;
             const int k = BKF ? e % BK : e / BN, j = BKF ? e / BK : e % BN;
-            Bs[buf * BK * BP + k * BP + j] = rb[q];
+            double v = rb[q];
+            if constexpr (!std::is_same<SB, Ident>::value) {
+                const int gk = fk0 + k, gj = fn0 + j;
+                v = (gk < K && gj < N) ? sb(gk, gj, v) : 0.0;
+            }
+            Bs[buf * BK * BP + k * BP + j] = v;
         }
     };
     double cpre[TM][TN];
@@ -323,11 +344,13 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
     }
 }
 
-template <class T, bool AMF, bool BKF, class LA, class LB, class ST>
-__device__ __forceinline__ void gemm(int M, int N, int K, LA la, LB lb, ST st, double *sm)
+template <class T, bool AMF, bool BKF, class LA, class LB, class ST, class SA = Ident,
+          class SB = Ident>
+__device__ __forceinline__ void gemm(int M, int N, int K, LA la, LB lb, ST st, double *sm,
+                                     SA sa = SA(), SB sb = SB())
 {
     gemm_core<T, AMF, BKF, false>(
-        M, N, K, la, lb, [](int, int) { return 0.0; }, st, sm);
+        M, N, K, la, lb, [](int, int) { return 0.0; }, st, sm, sa, sb);
 }
 
 /* C(i,j) <- st(i, j, sum_k a b, C(i,j)) with C read through lc */
@@ -339,16 +362,16 @@ __device__ __forceinline__ void gemm_rmw(int M, int N, int K, LA la, LB lb, LC l
 }
 
 /* Square-product dispatch by size: small lattices use 32x32 tiles. */
-template <bool AMF, bool BKF, class LA, class LB, class ST>
+template <bool AMF, bool BKF, class LA, class LB, class ST, class SA = Ident, class SB = Ident>
 __device__ __forceinline__ void gemm_sq(int M, int N, int K, LA la, LB lb, ST st,
-                                        double *sm)
+                                        double *sm, SA sa = SA(), SB sb = SB())
 {
     if (M <= 32 && N <= 32)
-        gemm<TSm, AMF, BKF>(M, N, K, la, lb, st, sm);
+        gemm<TSm, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
     else if (M <= 64)
-        gemm<TMma, AMF, BKF>(M, N, K, la, lb, st, sm);
+        gemm<TMma, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
     else
-        gemm<TSquare, AMF, BKF>(M, N, K, la, lb, st, sm);
+        gemm<TSquare, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
 }
 
 /* ------------------------------------------------------------ workspace */
@@ -1361,13 +1384,14 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
     if (B != nullptr) {
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return B[i + (size_t)k * n]; },
-            [=](int k, int j) { return U[k + (size_t)j * n] * eD[j]; },
-            [=](int i, int j, double v) { M[i + (size_t)j * n] = v; }, s.gsm);
+            [=](int k, int j) { return U[k + (size_t)j * n]; },
+            [=](int i, int j, double v) { M[i + (size_t)j * n] = v * eD[j]; }, s.gsm);
     } else {
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-            [=](int k, int j) { return vl[k] * U[k + (size_t)j * n] * eD[j]; },
-            [=](int i, int j, double v) { M[i + (size_t)j * n] = v; }, s.gsm);
+            [=](int k, int j) { return U[k + (size_t)j * n]; },
+            [=](int i, int j, double v) { M[i + (size_t)j * n] = v * eD[j]; }, s.gsm, Ident(),
+            [=](int k, int, double x) { return vl[k] * x; });
     }
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
@@ -1376,11 +1400,13 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
     const double *T = u.T;
     const int *perm = s.perm;
     double *Tn = w.m2;
+    double *rd = s.vD;
+    for (int i = threadIdx.x; i < n; i += NT) rd[i] = R[i + (size_t)i * n];
+    __syncthreads();
     gemm_sq<true, true>(
-        n, n, n,
-        [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] / R[i + (size_t)i * n] : 0.0; },
+        n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
         [=](int k, int j) { return T[perm[k] + (size_t)j * n]; },
-        [=](int i, int j, double v) { Tn[i + (size_t)j * n] = v; }, s.gsm);
+        [=](int i, int j, double v) { Tn[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
     for (int e = threadIdx.x; e < n * n; e += NT) u.T[e] = Tn[e];
     qr_form_q(n, w.m1, w.tw, u.U, s);
     for (int e = threadIdx.x; e < n * n; e += NT) u.U[e] *= s.vC[e / n];
@@ -1398,9 +1424,9 @@ __device__ __noinline__ void udv_rmul(int n, Udv u, const double *B, Scr w, Smem
     const double *eD = s.vA;
     double *M = w.m0;
     gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return eD[i] * T[i + (size_t)k * n]; },
+        n, n, n, [=](int i, int k) { return T[i + (size_t)k * n]; },
         [=](int k, int j) { return B[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { M[i + (size_t)j * n] = v; }, s.gsm);
+        [=](int i, int j, double v) { M[i + (size_t)j * n] = eD[i] * v; }, s.gsm);
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
     const int sg = qr_diag(n, w.m1, s, flag);
@@ -1467,11 +1493,13 @@ __device__ __noinline__ void udv_combine(int n, Udv l, Udv r, Udv o, Scr w, Smem
     const double *R = w.m1, *TR = r.T;
     const int *perm = s.perm;
     double *To = o.T;
+    double *rd = s.vD;
+    for (int i = threadIdx.x; i < n; i += NT) rd[i] = R[i + (size_t)i * n];
+    __syncthreads();
     gemm_sq<true, true>(
-        n, n, n,
-        [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] / R[i + (size_t)i * n] : 0.0; },
+        n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
         [=](int k, int j) { return TR[perm[k] + (size_t)j * n]; },
-        [=](int i, int j, double v) { To[i + (size_t)j * n] = v; }, s.gsm);
+        [=](int i, int j, double v) { To[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
     for (int i = threadIdx.x; i < n; i += NT) o.ell[i] = s.vB[i];
     if (threadIdx.x == 0) *o.det = *l.det * ((nt & 1) ? -1.0 : 1.0) * sg;
     __syncthreads();
@@ -1521,8 +1549,9 @@ __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const dou
     }
     gemm_sq<true, true>(
         n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-        [=](int k, int j) { return vv[k] * G[k + (size_t)j * n] * vi[j]; },
-        [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; }, s.gsm);
+        [=](int k, int j) { return G[k + (size_t)j * n]; },
+        [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v * vi[j]; }, s.gsm, Ident(),
+        [=](int k, int, double x) { return vv[k] * x; });
     gemm_sq<true, true>(
         n, n, n, [=](int i, int k) { return tmp[i + (size_t)k * n]; },
         [=](int k, int j) { return expKinv[k + (size_t)j * n]; },
@@ -1547,8 +1576,9 @@ __device__ __noinline__ void bblock(int n, int l0, int len, const signed char *f
         for (int k = threadIdx.x; k < n; k += NT) vv[k] = fp[k] > 0 ? v1 : v0;
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-            [=](int k, int j) { return vv[k] * src[k + (size_t)j * n]; },
-            [=](int i, int j, double v) { dst[i + (size_t)j * n] = v; }, s.gsm);
+            [=](int k, int j) { return src[k + (size_t)j * n]; },
+            [=](int i, int j, double v) { dst[i + (size_t)j * n] = v; }, s.gsm, Ident(),
+            [=](int k, int, double x) { return vv[k] * x; });
         src = dst;
     }
 }

@@ -153,13 +153,10 @@ __device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *
     __syncthreads();
     /* Zs = (E_A - G[:,A]) Tu F  (n x m),  Ys = Tv^T G[A,:]  (m x n) */
     gemm_sq<true, true>(
-        n, m, m,
-        [=](int i, int k) {
-            const int col = i0 + alist[k];
-            return (i == col ? 1.0 : 0.0) - G[i + (size_t)col * n];
-        },
+        n, m, m, [=](int i, int k) { return G[i + (size_t)(i0 + alist[k]) * n]; },
         [=](int k, int j) { return Tu[k * LD + j]; },
-        [=](int i, int j, double v) { Zs[i + (size_t)j * n] = v * facs[j]; }, s.gsm);
+        [=](int i, int j, double v) { Zs[i + (size_t)j * n] = v * facs[j]; }, s.gsm,
+        [=](int i, int k, double x) { return (i == i0 + alist[k] ? 1.0 : 0.0) - x; });
     gemm<TMmaWide, false, true>(
         m, n, m, [=](int i, int k) { return Tv[k * LD + i]; },
         [=](int k, int j) { return G[(i0 + alist[k]) + (size_t)j * n]; },
