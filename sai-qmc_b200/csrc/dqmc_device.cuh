@@ -498,6 +498,27 @@ __device__ inline Smem carve(double *base, int n, int kb)
     return s;
 }
 
+/* Elementwise pass over e < count with U loads in flight per thread:
+ * ld(e) for a batch of U elements first, then st(e, value) for each, so
+ * no load waits behind a store the compiler cannot prove independent. */
+template <int U = 8, class LD, class ST>
+__device__ __forceinline__ void ew_batched(int count, LD ld, ST st)
+{
+    for (int e0 = threadIdx.x; e0 < count; e0 += NT * U) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * NT;
+            v[u] = e < count ? ld(e) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * NT;
+            if (e < count) st(e, v[u]);
+        }
+    }
+}
+
 /* Per-chain error flag kept in shared memory (bit-or of DQMC_ST_*). */
 __device__ __forceinline__ void raise_flag(int *flag, int bit)
 {
@@ -1346,10 +1367,10 @@ __device__ void udv_identity(Udv u, int n)
 
 __device__ void udv_copy(Udv d, Udv s, int n)
 {
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        d.U[e] = s.U[e];
-        d.T[e] = s.T[e];
-    }
+    const double *sU = s.U, *sT = s.T;
+    double *dU = d.U, *dT = d.T;
+    ew_batched(n * n, [=](int e) { return sU[e]; }, [=](int e, double x) { dU[e] = x; });
+    ew_batched(n * n, [=](int e) { return sT[e]; }, [=](int e, double x) { dT[e] = x; });
     for (int i = threadIdx.x; i < n; i += NT) d.ell[i] = s.ell[i];
     if (threadIdx.x == 0) *d.det = *s.det;
     __syncthreads();
@@ -1407,9 +1428,18 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
         n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
         [=](int k, int j) { return T[perm[k] + (size_t)j * n]; },
         [=](int i, int j, double v) { Tn[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
-    for (int e = threadIdx.x; e < n * n; e += NT) u.T[e] = Tn[e];
+    {
+        double *uT = u.T;
+        const double *tn = Tn;
+        ew_batched(n * n, [=](int e) { return tn[e]; }, [=](int e, double x) { uT[e] = x; });
+    }
     qr_form_q(n, w.m1, w.tw, u.U, s);
-    for (int e = threadIdx.x; e < n * n; e += NT) u.U[e] *= s.vC[e / n];
+    {
+        double *uU = u.U;
+        const double *sg = s.vC;
+        ew_batched(n * n, [=](int e) { return uU[e]; },
+                   [=](int e, double x) { uU[e] = x * sg[e / n]; });
+    }
     for (int i = threadIdx.x; i < n; i += NT) u.ell[i] = s.vB[i];
     if (threadIdx.x == 0) *u.det = ((nt & 1) ? -1.0 : 1.0) * sg;
     __syncthreads();
@@ -1446,10 +1476,17 @@ __device__ __noinline__ void udv_rmul(int n, Udv u, const double *B, Scr w, Smem
         for (int e = threadIdx.x; e < n * n; e += NT) u.U[e] = Un[e];
     }
     const double *R = w.m1;
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e % n, r = e / n;
-        u.T[i + (size_t)s.perm[r] * n] =
-            r >= i ? R[i + (size_t)r * n] / R[i + (size_t)i * n] : 0.0;
+    {
+        double *rd = s.vD, *uT = u.T;
+        const int *perm = s.perm;
+        for (int i = threadIdx.x; i < n; i += NT) rd[i] = R[i + (size_t)i * n];
+        __syncthreads();
+        ew_batched(
+            n * n, [=](int e) { return (e % n) <= (e / n) ? R[e] : 0.0; },
+            [=](int e, double x) {
+                const int i = e % n, r = e / n;
+                uT[i + (size_t)perm[r] * n] = r >= i ? x / rd[i] : 0.0;
+            });
     }
     for (int i = threadIdx.x; i < n; i += NT) u.ell[i] = s.vB[i];
     __syncthreads();
@@ -1514,15 +1551,48 @@ __device__ __noinline__ int udv_green(int n, Udv u, double *G, Scr w, Smem &s, i
 {
     const double *U = u.U, *T = u.T, *ell = u.ell;
     double *X = w.m1, *Y = w.m0;
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e % n, j = e / n;
+    double *dbi = s.vA, *dsm = s.vB;
+    for (int i = threadIdx.x; i < n; i += NT) {
         const double l = ell[i];
-        const double dbi = exp(-fmax(l, 0.0)), ds = exp(fmin(l, 0.0));
-        const double ut = U[j + (size_t)i * n];
-        Y[e] = dbi * ut;
-        X[e] = dbi * ut + ds * T[e];
+        dbi[i] = exp(-fmax(l, 0.0));
+        dsm[i] = exp(fmin(l, 0.0));
     }
     __syncthreads();
+    if (s.q.cb >= 32) {
+        /* U^T through shared memory, 32 columns of U at a time: columns of U
+         * are read and rows of Y / X written in contiguous runs */
+        const int lds = n + 1;
+        double *S = s.q.X;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int nc = min(32, n - c0);
+            ew_batched(n * 32, [=](int e) {
+                const int j = e % n, c = e / n;
+                return c < nc ? U[j + (size_t)(c0 + c) * n] : 0.0;
+            }, [=](int e, double x) { S[(e % n) + (e / n) * lds] = x; });
+            __syncthreads();
+            ew_batched(n * 32, [=](int e) {
+                const int c = e & 31, j = e >> 5;
+                return c < nc ? T[(c0 + c) + (size_t)j * n] : 0.0;
+            }, [=](int e, double t) {
+                const int c = e & 31, j = e >> 5;
+                if (c < nc) {
+                    const int i = c0 + c;
+                    const double y = dbi[i] * S[j + c * lds];
+                    Y[i + (size_t)j * n] = y;
+                    X[i + (size_t)j * n] = y + dsm[i] * t;
+                }
+            });
+            __syncthreads();
+        }
+    } else {
+        for (int e = threadIdx.x; e < n * n; e += NT) {
+            const int i = e % n, j = e / n;
+            const double ut = U[j + (size_t)i * n];
+            Y[e] = dbi[i] * ut;
+            X[e] = dbi[i] * ut + dsm[i] * T[e];
+        }
+        __syncthreads();
+    }
     const int nt = qr_factor(n, X, w.tw, s, flag);
     const int sg = qr_diag(n, X, s, flag);
     qr_apply_qt(n, X, w.tw, Y, n, s);
@@ -1547,11 +1617,15 @@ __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const dou
         vv[k] = up ? v1 : v0;
         vi[k] = up ? vi1 : vi0;
     }
+    __syncthreads();
+    /* G <- diag(v) G diag(1/v) in place (G is overwritten below), so both
+     * products are plain */
+    ew_batched(n * n, [=](int e) { return G[e]; },
+               [=](int e, double x) { G[e] = x * (vv[e % n] * vi[e / n]); });
     gemm_sq<true, true>(
         n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
         [=](int k, int j) { return G[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v * vi[j]; }, s.gsm, Ident(),
-        [=](int k, int, double x) { return vv[k] * x; });
+        [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; }, s.gsm);
     gemm_sq<true, true>(
         n, n, n, [=](int i, int k) { return tmp[i + (size_t)k * n]; },
         [=](int k, int j) { return expKinv[k + (size_t)j * n]; },
@@ -1562,23 +1636,32 @@ __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const dou
 __device__ __noinline__ void bblock(int n, int l0, int len, const signed char *field, const double *expK,
                        double v0, double v1, double *out, double *X, double *Y, Smem &s)
 {
+    /* Intermediate products are stored row-scaled by the next slice's
+     * diag(v) (folded into the producing GEMM's epilogue), so every
+     * product is a plain expK * X. */
     const signed char *f0 = field + (size_t)l0 * n;
     double *first = (len == 1) ? out : X;
-    for (int e = threadIdx.x; e < n * n; e += NT)
-        first[e] = expK[e] * (f0[e / n] > 0 ? v1 : v0);
+    double *vv = s.vA;
+    for (int i = threadIdx.x; i < n; i += NT)
+        vv[i] = (len == 1) ? 1.0 : (field[(size_t)(l0 + 1) * n + i] > 0 ? v1 : v0);
+    __syncthreads();
+    ew_batched(n * n, [=](int e) { return expK[e]; }, [=](int e, double x) {
+        first[e] = vv[e % n] * (x * (f0[e / n] > 0 ? v1 : v0));
+    });
     __syncthreads();
     const double *src = first;
-    double *vv = s.vA;
     for (int p = 1; p < len; ++p) {
-        double *dst = (p == len - 1) ? out : ((src == X) ? Y : X);
-        const signed char *fp = field + (size_t)(l0 + p) * n;
-        __syncthreads();
-        for (int k = threadIdx.x; k < n; k += NT) vv[k] = fp[k] > 0 ? v1 : v0;
+        const bool lastp = (p == len - 1);
+        double *dst = lastp ? out : ((src == X) ? Y : X);
+        if (!lastp) {
+            const signed char *fn = field + (size_t)(l0 + p + 1) * n;
+            for (int i = threadIdx.x; i < n; i += NT) vv[i] = fn[i] > 0 ? v1 : v0;
+        }
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
             [=](int k, int j) { return src[k + (size_t)j * n]; },
-            [=](int i, int j, double v) { dst[i + (size_t)j * n] = v; }, s.gsm, Ident(),
-            [=](int k, int, double x) { return vv[k] * x; });
+            [=](int i, int j, double v) { dst[i + (size_t)j * n] = lastp ? v : vv[i] * v; },
+            s.gsm);
         src = dst;
     }
 }

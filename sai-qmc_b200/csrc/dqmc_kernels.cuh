@@ -174,10 +174,23 @@ __device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *
 __device__ double adopt_green(int n, double *G, const double *Gn, Smem &s)
 {
     double mx = 0.0;
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        const double d = fabs(G[e] - Gn[e]);
-        mx = (d > mx || d != d) ? d : mx;
-        G[e] = Gn[e];
+    for (int e0 = threadIdx.x; e0 < n * n; e0 += NT * 8) {
+        double a[8], b[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * NT;
+            a[u] = e < n * n ? G[e] : 0.0;
+            b[u] = e < n * n ? Gn[e] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * NT;
+            if (e < n * n) {
+                const double d = fabs(a[u] - b[u]);
+                mx = (d > mx || d != d) ? d : mx;
+                G[e] = b[u];
+            }
+        }
     }
     return block_reduce<true>(mx, s.red);
 }
