@@ -102,14 +102,21 @@ using TMmaWide = Tile<16, 128, 16, 2, 4, true, 1>;
 /* 128 x 64 with 2 x 4 warps: 4 x 2 fragments per warp, twice the
  * independent accumulators per warp (needs the full register file) */
 using TMmaBig = Tile<128, 64, 16, 8, 4, true, 2>;
+/* 128 x 128 with 2 x 4 warps: 4 x 4 fragments (16 accumulators) per warp,
+ * for products without a read-modify-write epilogue */
+using TMmaWideSq = Tile<128, 128, 16, 16, 4, true, 2>;
 #if DQMC_MINB == 1
 using TSquare = TMmaBig;
+using TSquareNR = TMmaWideSq;
 #else
 using TSquare = TMma;
+using TSquareNR = TMma;
 #endif
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
-constexpr int GEMM_SMEM = cmax(cmax(TWide::SMEM, TSq::SMEM),
-                               cmax(cmax(TMma::SMEM, TMmaWide::SMEM), TSquare::SMEM));
+constexpr int GEMM_SMEM =
+    cmax(cmax(TWide::SMEM, TSq::SMEM),
+         cmax(cmax(TMma::SMEM, TMmaWide::SMEM), cmax(TSquare::SMEM, TSquareNR::SMEM)));
+
 
 /* D = A(16xKS) B(KSx8) + C, FP64 on the tensor cores.  Fragments: lane
  * (gid = lane/4, tig = lane%4) holds a[2q] = A(gid, tig+4q), a[2q+1] =
@@ -370,8 +377,30 @@ __device__ __forceinline__ void gemm_sq(int M, int N, int K, LA la, LB lb, ST st
         gemm<TSm, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
     else if (M <= 64)
         gemm<TMma, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
+    else if (N > 64)
+        gemm<TSquareNR, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
     else
         gemm<TSquare, AMF, BKF>(M, N, K, la, lb, st, sm, sa, sb);
+}
+
+/* C = A B for column-major A (lda) and B (ldb), epilogue st(i, j, acc). */
+template <class ST>
+__device__ __forceinline__ void gemm_nn(int M, int N, int K, const double *A, int lda,
+                                        const double *B, int ldb, ST st, double *sm)
+{
+    gemm_sq<true, true>(
+        M, N, K, [=](int i, int k) { return A[i + (size_t)k * lda]; },
+        [=](int k, int j) { return B[k + (size_t)j * ldb]; }, st, sm);
+}
+
+/* C(i, j) <- st(i, j, (A B)(i, j), C(i, j)), C read through lc. */
+template <class LC, class ST>
+__device__ __forceinline__ void gemm_nn_rmw(int M, int N, int K, const double *A, int lda,
+                                            const double *B, int ldb, LC lc, ST st, double *sm)
+{
+    gemm_rmw<TSquare, true, true>(
+        M, N, K, [=](int i, int k) { return A[i + (size_t)k * lda]; },
+        [=](int k, int j) { return B[k + (size_t)j * ldb]; }, lc, st, sm);
 }
 
 /* ------------------------------------------------------------ workspace */
@@ -400,9 +429,12 @@ __host__ __device__ inline size_t smem_fixed(int n)
     const size_t ints = (size_t)n + 2 * DQMC_MAX_KB + 8;
     return ((40 + 4 * (size_t)n + (ints + 1) / 2) + 1) & ~(size_t)1;
 }
-__host__ __device__ inline size_t smem_gemm_union(int n)
+/* GEMM staging + the phase area behind it: with the shared-memory QR
+ * (cb > 0) the phase area holds the site block or a 16 x 16 triangle
+ * block; otherwise also the global-memory QR's panel. */
+__host__ __device__ inline size_t smem_gemm_union(int n, int cb)
 {
-    const size_t qr = (size_t)n * QNB + (size_t)QNB * WCOLS + 2 * QNB * QNB + QNB;
+    const size_t qr = cb ? 256 : (size_t)n * QNB + (size_t)QNB * WCOLS + 2 * QNB * QNB + QNB;
     const size_t pr = 4 * (size_t)DQMC_MAX_KB * (DQMC_MAX_KB + 1) + DQMC_MAX_KB;
     return (size_t)GEMM_SMEM + (qr > pr ? qr : pr);
 }
@@ -410,7 +442,7 @@ __host__ __device__ inline int qr_cb(int n)
 {
     if (n > 3 * NT) return 0;
     const size_t base = smem_fixed(n) + 8;
-    const size_t gu = smem_gemm_union(n);
+    const size_t gu = smem_gemm_union(n, 16);
     for (int cb = 64; cb >= 16; cb -= 16) {
         const size_t q = qr_sm_doubles(n, cb);
         if (base + (q > gu ? q : gu) <= SMEM_BUDGET) return cb;
@@ -453,7 +485,7 @@ __host__ __device__ inline size_t smem_doubles(int n, int kb)
 {
     (void)kb;
     const int cb = qr_cb(n);
-    const size_t gu = smem_gemm_union(n);
+    const size_t gu = smem_gemm_union(n, cb);
     const size_t q = cb ? qr_sm_doubles(n, cb) : 0;
     return smem_fixed(n) + (q > gu ? q : gu) + 8;
 }
@@ -726,7 +758,7 @@ __device__ __noinline__ void trsm_upper(int n, const double *A, const double *Y,
                 X[(i0 + i) + (size_t)j * n] = Y[(i0 + i) + (size_t)j * n];
             }
         }
-        double *Rb = s.Tw;
+        double *Rb = s.phase;
         for (int e = threadIdx.x; e < QNB * QNB; e += NT) {
             const int i = e % QNB, k = e / QNB;
             Rb[e] = (i < bs && k < bs) ? A[(i0 + i) + (size_t)(i0 + k) * n] : 0.0;
@@ -1403,10 +1435,8 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
     double *eD = s.vA, *vl = s.vD;
     double *M = w.m0;
     if (B != nullptr) {
-        gemm_sq<true, true>(
-            n, n, n, [=](int i, int k) { return B[i + (size_t)k * n]; },
-            [=](int k, int j) { return U[k + (size_t)j * n]; },
-            [=](int i, int j, double v) { M[i + (size_t)j * n] = v * eD[j]; }, s.gsm);
+        gemm_nn(n, n, n, B, n, U, n,
+                [=](int i, int j, double v) { M[i + (size_t)j * n] = v * eD[j]; }, s.gsm);
     } else {
         gemm_sq<true, true>(
             n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
@@ -1453,10 +1483,8 @@ __device__ __noinline__ void udv_rmul(int n, Udv u, const double *B, Scr w, Smem
     const double *T = u.T;
     const double *eD = s.vA;
     double *M = w.m0;
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return T[i + (size_t)k * n]; },
-        [=](int k, int j) { return B[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { M[i + (size_t)j * n] = eD[i] * v; }, s.gsm);
+    gemm_nn(n, n, n, T, n, B, n,
+            [=](int i, int j, double v) { M[i + (size_t)j * n] = eD[i] * v; }, s.gsm);
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
     const int sg = qr_diag(n, w.m1, s, flag);
@@ -1507,11 +1535,9 @@ __device__ __noinline__ void udv_combine(int n, Udv l, Udv r, Udv o, Scr w, Smem
     double *M = w.m0;
     {
         const double *eR = s.vD;
-        gemm_sq<true, true>(
-            n, n, n, [=](int i, int k) { return TL[i + (size_t)k * n]; },
-            [=](int k, int j) { return UR[k + (size_t)j * n]; },
-            [=](int i, int j, double v) { M[i + (size_t)j * n] = eL[i] * v * eR[j]; },
-            s.gsm);
+        gemm_nn(n, n, n, TL, n, UR, n,
+                [=](int i, int j, double v) { M[i + (size_t)j * n] = eL[i] * v * eR[j]; },
+                s.gsm);
     }
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
@@ -1622,14 +1648,10 @@ __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const dou
      * products are plain */
     ew_batched(n * n, [=](int e) { return G[e]; },
                [=](int e, double x) { G[e] = x * (vv[e % n] * vi[e / n]); });
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-        [=](int k, int j) { return G[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; }, s.gsm);
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return tmp[i + (size_t)k * n]; },
-        [=](int k, int j) { return expKinv[k + (size_t)j * n]; },
-        [=](int i, int j, double v) { G[i + (size_t)j * n] = v; }, s.gsm);
+    gemm_nn(n, n, n, expK, n, G, n, [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; },
+            s.gsm);
+    gemm_nn(n, n, n, tmp, n, expKinv, n,
+            [=](int i, int j, double v) { G[i + (size_t)j * n] = v; }, s.gsm);
 }
 
 /* out = B_{l0+len-1} ... B_{l0} (green.c:151-166); X, Y ping-pong scratch. */
@@ -1657,11 +1679,9 @@ __device__ __noinline__ void bblock(int n, int l0, int len, const signed char *f
             const signed char *fn = field + (size_t)(l0 + p + 1) * n;
             for (int i = threadIdx.x; i < n; i += NT) vv[i] = fn[i] > 0 ? v1 : v0;
         }
-        gemm_sq<true, true>(
-            n, n, n, [=](int i, int k) { return expK[i + (size_t)k * n]; },
-            [=](int k, int j) { return src[k + (size_t)j * n]; },
-            [=](int i, int j, double v) { dst[i + (size_t)j * n] = lastp ? v : vv[i] * v; },
-            s.gsm);
+        gemm_nn(n, n, n, expK, n, src, n,
+                [=](int i, int j, double v) { dst[i + (size_t)j * n] = lastp ? v : vv[i] * v; },
+                s.gsm);
         src = dst;
     }
 }

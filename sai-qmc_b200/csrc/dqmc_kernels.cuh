@@ -162,10 +162,8 @@ __device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *
         [=](int k, int j) { return G[(i0 + alist[k]) + (size_t)j * n]; },
         [=](int i, int j, double v) { Ys[i + (size_t)j * kb] = v; }, s.gsm);
     /* G -= Zs Ys */
-    gemm_rmw<TSquare, true, true>(
-        n, n, m, [=](int i, int k) { return Zs[i + (size_t)k * n]; },
-        [=](int k, int j) { return Ys[k + (size_t)j * kb]; },
-        [=](int i, int j) { return G[i + (size_t)j * n]; },
+    gemm_nn_rmw(
+        n, n, m, Zs, n, Ys, kb, [=](int i, int j) { return G[i + (size_t)j * n]; },
         [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
     pc.charge(ch, DQMC_PH_FLUSH);
 }
