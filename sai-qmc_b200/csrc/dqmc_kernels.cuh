@@ -126,24 +126,26 @@ __device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *
      * row q.  Su[r][p] = V[i_p, r] = Rrow[r][a_p], Sc[r][p] = C[i_p, r] =
      * -fac_r Ccol[r][a_p], both for r < p. */
     if (warp < 2) {
-        double xr[KB];
+        /* right-looking: once xr[r] is final its contribution goes to every
+         * later p, so each of the m steps is a row of independent FMAs */
+        const double *Src = (warp == 0) ? Rrow : Ccol;
         const int q = lane;
+        int ap[KB];
+        double xr[KB];
 #pragma unroll
         for (int p = 0; p < KB; ++p) {
-            double v = 0.0;
-            if (p < m && q <= p) {
-                v = (q == p) ? 1.0 : 0.0;
-                const int ap = alist[p];
+            ap[p] = p < m ? alist[p] : 0;
+            xr[p] = (p == q) ? 1.0 : 0.0;
+        }
 #pragma unroll
-                for (int r = 0; r < p; ++r) {
-                    if (r >= q) {
-                        const double nrp = (warp == 0) ? -facs[r] * Rrow[r * LD + ap]
-                                                       : -facs[r] * Ccol[r * LD + ap];
-                        v -= xr[r] * nrp;
-                    }
-                }
+        for (int r = 0; r < KB - 1; ++r) {
+            if (r + 1 < m) {
+                const double c = xr[r] * facs[r];
+                const double *row = Src + r * LD;
+#pragma unroll
+                for (int p = r + 1; p < KB; ++p)
+                    if (p < m) xr[p] = fma(c, row[ap[p]], xr[p]);
             }
-            xr[p] = v;
         }
         double *T = (warp == 0) ? Tu : Tv;
 #pragma unroll
