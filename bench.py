@@ -25,6 +25,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "sai-qmc_b200")
 for _p in (ROOT, PKG):
@@ -312,6 +314,46 @@ def e2e_run(steps, warmup, chains, precision):
                     "host<->device copies divided by its sweeps"}
 
 
+def precision_compare(dq, chains, args, precision, value):
+    """The other precision mode on the same workload (same chains, warm-up
+    and timed sweeps), and a same-seed check between the two: 4 chains x 2
+    sweeps from identical fields, field flips compared, max|G_mixed -
+    G_FP64| after the sweeps (G is rebuilt from the FP64 stack at every
+    stabilization point) and each mode's stabilization drift
+    max|G_wrapped - G_rebuilt|."""
+    other = dq.PREC_FP64 if precision == dq.PREC_MIXED else dq.PREC_MIXED
+    e = make_engine(dq, chains, 0, other)
+    e.prepare(1)
+    for _ in range(args.warmup):
+        e.sweep(1)
+    e.sync()
+    e.mark(0)
+    e.sweep(args.steps)
+    e.mark(1)
+    ms = e.elapsed_ms() / args.steps
+    e.close()
+    other_value = chains * N_SITES * L_SLICES / (ms * 1e-3)
+    fp64_v, mixed_v = (value, other_value) if precision == dq.PREC_FP64 else (other_value, value)
+    ea = make_engine(dq, 4, 0, dq.PREC_FP64)
+    eb = make_engine(dq, 4, 0, dq.PREC_MIXED)
+    ea.prepare(1)
+    eb.prepare(1)
+    ea.sweep(2)
+    eb.sweep(2)
+    same = all(np.array_equal(ea.field(c), eb.field(c)) for c in range(4))
+    dg = max(float(np.max(np.abs(ea.green(c) - eb.green(c)))) for c in range(4))
+    drift = {"fp64": max(ea.counters(c)["drift_max"] for c in range(4)),
+             "mixed": max(eb.counters(c)["drift_max"] for c in range(4))}
+    ea.close()
+    eb.close()
+    return {"fp64_value": fp64_v, "mixed_value": mixed_v, "mixed_over_fp64": mixed_v / fp64_v,
+            "mixed": "wrap products as 6-digit int8 split products (mma.sync s8), "
+                     "stabilization, B-blocks, flushes and ratios FP64",
+            "same_seed_check": {"chains": 4, "sweeps": 2, "identical_flips": same,
+                                "max_abs_dG_after_sweeps": dg,
+                                "stabilization_drift_max": drift}}
+
+
 def run_gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -415,6 +457,8 @@ def run_gpu_arm(args):
             "chains_failed": status_bad,
             "measure_ms_per_step": meas_ms / max(1, nmeas),
         }
+        if world == 1 and not args.no_compare:
+            line["precision_compare"] = precision_compare(dq, chains, args, precision, value)
         if not args.no_single_chain and world == 1:
             e1 = make_engine(dq, 1, 0, precision)
             e1.prepare(1)
@@ -447,6 +491,8 @@ def main():
     ap.add_argument("--chains", type=int, default=0, help="chains per GPU (0: 2 x SMs)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip timing the other precision mode and the same-seed check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single-chain", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe")

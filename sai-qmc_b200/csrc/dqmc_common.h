@@ -50,6 +50,9 @@ enum {
     DQMC_PH_COUNT
 };
 
+/* int8 digits per operand of a split product (42 bits) */
+#define DQMC_MIX_DIGITS 6
+
 typedef struct {
     int n, Lx, Ly;
     double U, dtau, mu;
@@ -61,6 +64,12 @@ typedef struct {
     const int *bipart;
     int nq_zz, nq_perp;
     const double *cos_zz, *cos_perp;   /* n x nq phase tables (structure_factor.c:182-199) */
+    /* split-product (mixed precision) operands: DQMC_MIX_DIGITS int8 digit
+     * slices of expK by rows ([i][k], ld mix_kp) and of expKinv by columns
+     * ([j][k]), with the power-of-two exponent of each row / column */
+    const signed char *mixK, *mixKinv;
+    const int *mixK_ex, *mixKinv_ex;
+    int mix_kp;
 } DqmcModelDev;
 
 typedef struct {
@@ -89,6 +98,10 @@ typedef struct {
     double *bins;              /* nbin x DQMC_BIN_FIELDS */
     double *bins_zz, *bins_perp;   /* nbin x nq */
     int nbin;
+    /* mixed precision: digit slices of one operand (DQMC_MIX_DIGITS x n x
+     * mix_kp bytes) and its n exponents; null in FP64 mode */
+    signed char *mix;
+    int *mix_ex;
     unsigned long long prof[DQMC_PH_COUNT];
 } DqmcChainDev;
 

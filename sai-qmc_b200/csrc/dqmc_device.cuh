@@ -411,6 +411,8 @@ __device__ __forceinline__ void gemm_nn_rmw(int M, int N, int K, const double *A
  * small scratch.  cb is the widest of 64/48/32/16 that fits the CTA's
  * shared-memory budget; 0 selects the global-memory QR. */
 constexpr int QW = 20;              /* leading dimension of W (16 rows) */
+/* staging of the split-product GEMM (dqmc_mixed.cuh), one-CTA build only */
+constexpr size_t MIX_SMEM_DOUBLES = (DQMC_MINB == 1) ? 2560 * DQMC_MIX_DIGITS : 0;
 constexpr size_t QR_MISC = 1920;    /* T, gram, taus, reductions        */
 constexpr size_t SMEM_BUDGET = (DQMC_MINB == 1 ? 227 * 1024 : 113 * 1024) / 8;
 
@@ -486,7 +488,8 @@ __host__ __device__ inline size_t smem_doubles(int n, int kb)
     (void)kb;
     const int cb = qr_cb(n);
     const size_t gu = smem_gemm_union(n, cb);
-    const size_t q = cb ? qr_sm_doubles(n, cb) : 0;
+    size_t q = cb ? qr_sm_doubles(n, cb) : 0;
+    if (cb && q < MIX_SMEM_DOUBLES) q = MIX_SMEM_DOUBLES;
     return smem_fixed(n) + (q > gu ? q : gu) + 8;
 }
 

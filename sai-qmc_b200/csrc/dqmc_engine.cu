@@ -220,6 +220,10 @@ dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
         set_err("device %d out of range (%d devices)", d.device, ndev);
         return nullptr;
     }
+    if (d.precision != DQMC_PREC_FP64 && d.precision != DQMC_PREC_MIXED) {
+        set_err("precision %d is neither DQMC_PREC_FP64 nor DQMC_PREC_MIXED", d.precision);
+        return nullptr;
+    }
     if (cudaSetDevice(d.device) != cudaSuccess) {
         set_err("cudaSetDevice(%d) failed", d.device);
         return nullptr;
@@ -337,6 +341,33 @@ int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
     return (int)e->chains.size() - 1;
 }
 
+/* Digit slices of a split-product operand (the device's mix_split, same
+ * arithmetic: X = trunc(x 2^(7S-e)) in base-128 digits, signed top digit): line l of M is row l (by_rows: M[l + k*n]) or column l
+ * (M[k + l*n]); out: DQMC_MIX_DIGITS x n x kp bytes, ex: line exponents. */
+static void mix_split_host(int n, int kp, const double *M, bool by_rows,
+                           std::vector<signed char> &out, std::vector<int> &ex)
+{
+    out.assign((size_t)DQMC_MIX_DIGITS * n * kp, 0);
+    ex.assign(n, 0);
+    for (int l = 0; l < n; ++l) {
+        auto val = [&](int k) { return by_rows ? M[l + (size_t)k * n] : M[k + (size_t)l * n]; };
+        double m = 0.0;
+        for (int k = 0; k < n; ++k) m = std::fmax(m, std::fabs(val(k)));
+        int e = 0;
+        if (m > 0.0) std::frexp(m, &e);
+        ex[l] = e;
+        const double sc = std::ldexp(1.0, 7 * DQMC_MIX_DIGITS - e);
+        for (int k = 0; k < n; ++k) {
+            const long long X = (long long)(val(k) * sc);
+            for (int p = 0; p < DQMC_MIX_DIGITS; ++p) {
+                const int sh = 7 * (DQMC_MIX_DIGITS - 1 - p);
+                const unsigned d = p == 0 ? (unsigned)(X >> sh) & 255u : (unsigned)(X >> sh) & 127u;
+                out[(size_t)p * n * kp + (size_t)l * kp + k] = (signed char)(unsigned char)d;
+            }
+        }
+    }
+}
+
 int dqmc_engine_prepare(dqmc_engine *e, int nbin)
 {
     if (!e || e->prepared) return set_err("dqmc_engine_prepare: engine missing or prepared");
@@ -344,17 +375,29 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     CU(cudaSetDevice(e->desc.device));
     e->nbin = nbin > 0 ? nbin : 1;
     /* models */
+    const bool mixed = e->desc.precision == DQMC_PREC_MIXED;
+    if (mixed) {
+        for (const HModel &m : e->models)
+            if (!dq::qr_cb(m.n))
+                return set_err("dqmc_engine_prepare: mixed precision needs n <= %d here (n = %d)",
+                               3 * DQMC_NT, m.n);
+    }
     size_t moff = 0;
-    std::vector<size_t> mo(e->models.size() * 6);
+    std::vector<size_t> mo(e->models.size() * 10);
     for (size_t k = 0; k < e->models.size(); ++k) {
         const HModel &m = e->models[k];
         const size_t nn = (size_t)m.n * m.n;
-        mo[6 * k + 0] = moff; moff += rup(nn * 8);
-        mo[6 * k + 1] = moff; moff += rup(nn * 8);
-        mo[6 * k + 2] = moff; moff += rup(nn * 8);
-        mo[6 * k + 3] = moff; moff += rup((size_t)m.n * 4);
-        mo[6 * k + 4] = moff; moff += rup(m.cos_zz.size() * 8 + 8);
-        mo[6 * k + 5] = moff; moff += rup(m.cos_perp.size() * 8 + 8);
+        const size_t mixb = mixed ? (size_t)DQMC_MIX_DIGITS * m.n * dq::mix_kp(m.n) : 0;
+        mo[10 * k + 0] = moff; moff += rup(nn * 8);
+        mo[10 * k + 1] = moff; moff += rup(nn * 8);
+        mo[10 * k + 2] = moff; moff += rup(nn * 8);
+        mo[10 * k + 3] = moff; moff += rup((size_t)m.n * 4);
+        mo[10 * k + 4] = moff; moff += rup(m.cos_zz.size() * 8 + 8);
+        mo[10 * k + 5] = moff; moff += rup(m.cos_perp.size() * 8 + 8);
+        mo[10 * k + 6] = moff; moff += rup(mixb + 8);
+        mo[10 * k + 7] = moff; moff += rup(mixb + 8);
+        mo[10 * k + 8] = moff; moff += rup((size_t)m.n * 4);
+        mo[10 * k + 9] = moff; moff += rup((size_t)m.n * 4);
     }
     const size_t mstruct = moff;
     moff += rup(sizeof(DqmcModelDev) * e->models.size());
@@ -383,25 +426,43 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
             d.Nup[is] = std::exp(-2.0 * lambda * 1.0 * sv) - 1.0;
             d.Ndn[is] = std::exp(-2.0 * lambda * -1.0 * sv) - 1.0;
         }
-        d.expK = (const double *)(e->dmod + mo[6 * k + 0]);
-        d.expKinv = (const double *)(e->dmod + mo[6 * k + 1]);
-        d.thop = (const double *)(e->dmod + mo[6 * k + 2]);
-        d.bipart = (const int *)(e->dmod + mo[6 * k + 3]);
-        d.cos_zz = (const double *)(e->dmod + mo[6 * k + 4]);
-        d.cos_perp = (const double *)(e->dmod + mo[6 * k + 5]);
+        d.expK = (const double *)(e->dmod + mo[10 * k + 0]);
+        d.expKinv = (const double *)(e->dmod + mo[10 * k + 1]);
+        d.thop = (const double *)(e->dmod + mo[10 * k + 2]);
+        d.bipart = (const int *)(e->dmod + mo[10 * k + 3]);
+        d.cos_zz = (const double *)(e->dmod + mo[10 * k + 4]);
+        d.cos_perp = (const double *)(e->dmod + mo[10 * k + 5]);
         d.nq_zz = m.nq_zz;
         d.nq_perp = m.nq_perp;
-        CU(cudaMemcpy(e->dmod + mo[6 * k + 0], m.expK.data(), nn * 8, cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->dmod + mo[6 * k + 1], m.expKinv.data(), nn * 8, cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->dmod + mo[6 * k + 2], m.thop.data(), nn * 8, cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(e->dmod + mo[6 * k + 3], m.bipart.data(), (size_t)m.n * 4,
+        CU(cudaMemcpy(e->dmod + mo[10 * k + 0], m.expK.data(), nn * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->dmod + mo[10 * k + 1], m.expKinv.data(), nn * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->dmod + mo[10 * k + 2], m.thop.data(), nn * 8, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->dmod + mo[10 * k + 3], m.bipart.data(), (size_t)m.n * 4,
                       cudaMemcpyHostToDevice));
         if (m.nq_zz)
-            CU(cudaMemcpy(e->dmod + mo[6 * k + 4], m.cos_zz.data(), m.cos_zz.size() * 8,
+            CU(cudaMemcpy(e->dmod + mo[10 * k + 4], m.cos_zz.data(), m.cos_zz.size() * 8,
                           cudaMemcpyHostToDevice));
         if (m.nq_perp)
-            CU(cudaMemcpy(e->dmod + mo[6 * k + 5], m.cos_perp.data(), m.cos_perp.size() * 8,
+            CU(cudaMemcpy(e->dmod + mo[10 * k + 5], m.cos_perp.data(), m.cos_perp.size() * 8,
                           cudaMemcpyHostToDevice));
+        if (mixed) {
+            const int kp = dq::mix_kp(m.n);
+            std::vector<signed char> sl;
+            std::vector<int> ex;
+            d.mix_kp = kp;
+            d.mixK = (const signed char *)(e->dmod + mo[10 * k + 6]);
+            d.mixKinv = (const signed char *)(e->dmod + mo[10 * k + 7]);
+            d.mixK_ex = (const int *)(e->dmod + mo[10 * k + 8]);
+            d.mixKinv_ex = (const int *)(e->dmod + mo[10 * k + 9]);
+            mix_split_host(m.n, kp, m.expK.data(), true, sl, ex);
+            CU(cudaMemcpy(e->dmod + mo[10 * k + 6], sl.data(), sl.size(), cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(e->dmod + mo[10 * k + 8], ex.data(), ex.size() * 4,
+                          cudaMemcpyHostToDevice));
+            mix_split_host(m.n, kp, m.expKinv.data(), false, sl, ex);
+            CU(cudaMemcpy(e->dmod + mo[10 * k + 7], sl.data(), sl.size(), cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(e->dmod + mo[10 * k + 9], ex.data(), ex.size() * 4,
+                          cudaMemcpyHostToDevice));
+        }
     }
     e->dmodels = (DqmcModelDev *)(e->dmod + mstruct);
     CU(cudaMemcpy(e->dmodels, hm.data(), sizeof(DqmcModelDev) * hm.size(),
@@ -430,6 +491,10 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
         off += rup((size_t)e->nbin * m.nq_perp * 8 + 8);
+        if (mixed) {
+            off += rup((size_t)DQMC_MIX_DIGITS * n * dq::mix_kp(n));   /* digit slices */
+            off += rup((size_t)n * 4);                                  /* exponents */
+        }
         const size_t sm = dq::smem_bytes(n, c.kb);
         if (sm > maxsmem) maxsmem = sm;
         const size_t sm2 = dq2x::smem_bytes(n, c.kb);
@@ -473,6 +538,10 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         d.bins = (double *)take((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         d.bins_zz = (double *)take((size_t)e->nbin * m.nq_zz * 8 + 8);
         d.bins_perp = (double *)take((size_t)e->nbin * m.nq_perp * 8 + 8);
+        if (mixed) {
+            d.mix = (signed char *)take((size_t)DQMC_MIX_DIGITS * n * dq::mix_kp(n));
+            d.mix_ex = (int *)take((size_t)n * 4);
+        }
         CU(cudaMemcpy(d.field, c.field.data(), c.field.size(), cudaMemcpyHostToDevice));
     }
     e->dchains = (DqmcChainDev *)(e->darena + cstruct);
@@ -491,7 +560,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         const bool fits2 = 2 * (e->smem2 + 1024) <= 228 * 1024;
         const int want = e->desc.ctas_per_sm;
-        e->per_sm = (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 ? 2 : 1;
+        e->per_sm = (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 && !mixed ? 2 : 1;
         if (e->per_sm == 2) CU(dq2x::set_attrs(e->smem2, e->msmem));
     }
     dq::k_init<<<(unsigned)nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels);
@@ -510,7 +579,8 @@ static int check_prepared(dqmc_engine *e, const char *who)
 
 static int kflags(const dqmc_engine *e)
 {
-    return (e->desc.drift & DQMC_DRIFT_SCRATCH) ? dq::KF_SDRIFT : 0;
+    return ((e->desc.drift & DQMC_DRIFT_SCRATCH) ? dq::KF_SDRIFT : 0) |
+           (e->desc.precision == DQMC_PREC_MIXED ? dq::KF_MIXED : 0);
 }
 
 int dqmc_sweep(dqmc_engine *e, int nsweeps)
@@ -754,7 +824,8 @@ int dqmc_wrap_green(dqmc_engine *e, int chain, int l, double *G)
     CU(cudaMalloc(&dG, bytes));
     cudaError_t err = cudaMemcpy(dG, G, bytes, cudaMemcpyHostToDevice);
     if (err == cudaSuccess) {
-        dq::k_wrap<<<1, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels, chain, l, dG);
+        dq::k_wrap<<<1, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels, chain, l, dG,
+                                                       kflags(e));
         err = cudaGetLastError();
     }
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);

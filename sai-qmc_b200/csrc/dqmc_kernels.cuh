@@ -1,10 +1,11 @@
 /* Sweep, measurement and test kernels.  One CTA = one chain. */
 #pragma once
 #include "dqmc_device.cuh"
+#include "dqmc_mixed.cuh"
 
 namespace DQMC_NS {
 
-enum { KF_MEASURE = 1, KF_SDRIFT = 2, KF_STAB_DRIFT = 4 };
+enum { KF_MEASURE = 1, KF_SDRIFT = 2, KF_STAB_DRIFT = 4, KF_MIXED = 8 };
 
 /* Phase timer: thread 0 charges the cycles since the last mark to a phase.
  * Phases end at a CTA barrier, so thread 0's clock covers all threads. */
@@ -262,8 +263,14 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         for (int i0 = 0; i0 < n; i0 += kb)
             site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs, ch->Ys,
                        s, ch, pc);
-        wrap_green(n, G, tmp, md.expK, md.expKinv, fl, v0, v1, md.expvinv[0], md.expvinv[1],
-                   s);
+#if DQMC_MINB == 1
+        if (kflags & KF_MIXED)
+            wrap_green_mixed(n, G, tmp, md, fl, v0, v1, md.expvinv[0], md.expvinv[1], ch->mix,
+                             ch->mix_ex, s);
+        else
+#endif
+            wrap_green(n, G, tmp, md.expK, md.expKinv, fl, v0, v1, md.expvinv[0],
+                       md.expvinv[1], s);
         pc.charge(ch, DQMC_PH_WRAP);
         const bool boundary = ((l + 1) % stab == 0) && (l + 1 < L);
         const bool last = (l + 1 == L);
@@ -398,13 +405,22 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
 }
 
 __global__ void __launch_bounds__(NT, DQMC_MINB)
-    k_wrap(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l, double *Gio)
+    k_wrap(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l, double *Gio,
+           int kflags)
 {
     extern __shared__ double smraw[];
     DqmcChainDev *ch = &chains[c];
     const DqmcModelDev &md = models[ch->model];
     Smem s = carve(smraw, ch->n, ch->kb);
     const int n = ch->n;
+#if DQMC_MINB == 1
+    if (kflags & KF_MIXED) {
+        wrap_green_mixed(n, Gio, ch->w[4], md, ch->field + (size_t)l * n, md.expv[0], md.expv[1],
+                         md.expvinv[0], md.expvinv[1], ch->mix, ch->mix_ex, s);
+        return;
+    }
+#endif
+    (void)kflags;
     wrap_green(n, Gio, ch->w[4], md.expK, md.expKinv, ch->field + (size_t)l * n, md.expv[0],
                md.expv[1], md.expvinv[0], md.expvinv[1], s);
 }
