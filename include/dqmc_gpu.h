@@ -28,6 +28,10 @@ extern "C" {
 typedef struct dqmc_engine dqmc_engine;
 
 enum { DQMC_PREC_FP64 = 0, DQMC_PREC_MIXED = 1 };
+/* Sweep order (DqmcSweepMode, src/dqmc.h:45-48): forward sweeps only, or
+ * alternating forward / backward sweeps carrying the prefix and suffix UDV
+ * stacks between them (src/dqmc.c:609-963). */
+enum { DQMC_SWEEP_FORWARD = 0, DQMC_SWEEP_ALTERNATING = 1 };
 enum { DQMC_DRIFT_STAB = 1, DQMC_DRIFT_SCRATCH = 2 };
 
 /* Per-bin scalar layout returned by dqmc_read_bins (src/replica.h:6-16). */
@@ -54,7 +58,8 @@ typedef struct {
                         (src/dqmc.c:64-98, costly)                            */
     int ctas_per_sm; /* sweep kernel residency: 0 = auto (two chains per SM
                         when there are more chains than SMs), 1 or 2      */
-    int reserved[7];
+    int sweep_order; /* DQMC_SWEEP_*                                        */
+    int reserved[6];
 } dqmc_engine_desc;
 
 typedef struct {

@@ -75,6 +75,10 @@ typedef struct {
 typedef struct {
     int model, n, L, stab, M, kb;
     int status, bvalid;        /* bvalid: cached B-block products are current */
+    /* alternating sweep order: direction of the next sweep (0 forward, 1
+     * backward) and whether the prefix stack P (after a forward sweep) or
+     * the suffix stack S (after a backward sweep) carries over */
+    int alt, dir, pvalid, svalid;
     double sign;
     unsigned long long attempts, accepted, sweeps;
     unsigned long long meas_accepted, meas_attempts;  /* counters at last measurement */
@@ -90,6 +94,7 @@ typedef struct {
     signed char *field;        /* L x n */
     double *G;                 /* n x n */
     double *S;                 /* (M+1) UDV slots */
+    double *P;                 /* (M+1) UDV slots, prefix stack (alternating) */
     double *left, *comb, *scr; /* UDV slots (scr: rebuilds from scratch) */
     double *bcache;            /* M x n x n block products B(b_{j+1}, b_j) */
     double *w[6];              /* n x n scratch */

@@ -1657,6 +1657,25 @@ __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const dou
             [=](int i, int j, double v) { G[i + (size_t)j * n] = v; }, s.gsm);
 }
 
+/* G <- B_l^{-1} G B_l = diag(1/v) expKinv G expK diag(v)
+ * (green_wrap_backward, green.c:529-548); the diagonals in the epilogue. */
+__device__ __noinline__ void wrap_green_back(int n, double *G, double *tmp, const double *expK,
+                                             const double *expKinv, const signed char *fl,
+                                             double v0, double v1, double vi0, double vi1,
+                                             Smem &s)
+{
+    double *vv = s.vA, *vi = s.vB;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        const bool up = fl[k] > 0;
+        vv[k] = up ? v1 : v0;
+        vi[k] = up ? vi1 : vi0;
+    }
+    gemm_nn(n, n, n, expKinv, n, G, n, [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; },
+            s.gsm);
+    gemm_nn(n, n, n, tmp, n, expK, n,
+            [=](int i, int j, double v) { G[i + (size_t)j * n] = (vi[i] * v) * vv[j]; }, s.gsm);
+}
+
 /* out = B_{l0+len-1} ... B_{l0} (green.c:151-166); X, Y ping-pong scratch. */
 __device__ __noinline__ void bblock(int n, int l0, int len, const signed char *field, const double *expK,
                        double v0, double v1, double *out, double *X, double *Y, Smem &s)

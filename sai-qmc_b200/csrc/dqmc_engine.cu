@@ -220,6 +220,11 @@ dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
         set_err("device %d out of range (%d devices)", d.device, ndev);
         return nullptr;
     }
+    if (d.sweep_order != DQMC_SWEEP_FORWARD && d.sweep_order != DQMC_SWEEP_ALTERNATING) {
+        set_err("sweep_order %d is neither DQMC_SWEEP_FORWARD nor DQMC_SWEEP_ALTERNATING",
+                d.sweep_order);
+        return nullptr;
+    }
     if (d.precision != DQMC_PREC_FP64 && d.precision != DQMC_PREC_MIXED) {
         set_err("precision %d is neither DQMC_PREC_FP64 nor DQMC_PREC_MIXED", d.precision);
         return nullptr;
@@ -376,6 +381,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     e->nbin = nbin > 0 ? nbin : 1;
     /* models */
     const bool mixed = e->desc.precision == DQMC_PREC_MIXED;
+    const bool alt = e->desc.sweep_order == DQMC_SWEEP_ALTERNATING;
     if (mixed) {
         for (const HModel &m : e->models)
             if (!dq::qr_cb(m.n))
@@ -483,6 +489,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += rup((size_t)c.L * n);                          /* field */
         off += rup(nn * 8);                                   /* G */
         off += rup((size_t)(c.M + 1) * usz * 8);              /* S */
+        if (alt) off += rup((size_t)(c.M + 1) * usz * 8);     /* P (alternating) */
         off += 3 * rup(usz * 8);                              /* left, comb, scr */
         off += rup((size_t)c.M * nn * 8);                     /* bcache */
         off += 6 * rup(nn * 8);                               /* w */
@@ -526,6 +533,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         d.field = (signed char *)take((size_t)c.L * n);
         d.G = (double *)take(nn * 8);
         d.S = (double *)take((size_t)(c.M + 1) * usz * 8);
+        if (alt) d.P = (double *)take((size_t)(c.M + 1) * usz * 8);
+        d.alt = alt ? 1 : 0;
         d.left = (double *)take(usz * 8);
         d.comb = (double *)take(usz * 8);
         d.scr = (double *)take(usz * 8);

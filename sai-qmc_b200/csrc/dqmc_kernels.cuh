@@ -234,28 +234,35 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
     double *G = ch->G, *Gn = ch->w[3], *tmp = ch->w[4], *tmp2 = ch->w[5];
     const double v0 = md.expv[0], v1 = md.expv[1];
     auto Sj = [&](int j) { return udv_at(ch->S + (size_t)j * usz, n); };
+    auto Pj = [&](int j) { return udv_at(ch->P + (size_t)j * usz, n); };
     Udv left = udv_at(ch->left, n), comb = udv_at(ch->comb, n);
+    const bool alt = ch->alt != 0;
     PhaseClock pc;
     pc.mark();
 
-    /* Block products B(b_{j+1}, b_j) of the current field.  After the first
-     * sweep they are the ones the previous sweep's left pass computed. */
-    if (!ch->bvalid) {
-        for (int j = 1; j < M; ++j) {
-            const int b0 = j * stab, b1 = min((j + 1) * stab, L);
-            bblock(n, b0, b1 - b0, ch->field, md.expK, v0, v1, ch->bcache + j * nn, tmp, tmp2,
-                   s);
+    /* alternating order with a suffix stack carried from the backward sweep
+     * before (dqmc.c:622-629): no stack build */
+    if (!(alt && ch->svalid)) {
+        /* Block products B(b_{j+1}, b_j) of the current field.  After the
+         * first sweep they are the ones the previous sweep computed. */
+        if (!ch->bvalid) {
+            for (int j = 1; j < M; ++j) {
+                const int b0 = j * stab, b1 = min((j + 1) * stab, L);
+                bblock(n, b0, b1 - b0, ch->field, md.expK, v0, v1, ch->bcache + j * nn, tmp,
+                       tmp2, s);
+            }
+        }
+        pc.charge(ch, DQMC_PH_BCACHE);
+        /* suffix stack (green_stack_build_suffix, green.c:203-226) */
+        udv_identity(Sj(M), n);
+        for (int j = M - 1; j >= 1; --j) {
+            udv_copy(Sj(j), Sj(j + 1), n);
+            udv_rmul(n, Sj(j), ch->bcache + j * nn, w, s, flag);
+            if (*flag) return false;
         }
     }
-    pc.charge(ch, DQMC_PH_BCACHE);
-    /* suffix stack (green_stack_build_suffix, green.c:203-226) */
-    udv_identity(Sj(M), n);
-    for (int j = M - 1; j >= 1; --j) {
-        udv_copy(Sj(j), Sj(j + 1), n);
-        udv_rmul(n, Sj(j), ch->bcache + j * nn, w, s, flag);
-        if (*flag) return false;
-    }
     udv_identity(left, n);
+    if (alt) udv_copy(Pj(0), left, n);   /* prefix stack (dqmc.c:648-650) */
     pc.charge(ch, DQMC_PH_STACK);
     int tau_left = 0;
     for (int l = 0; l < L; ++l) {
@@ -302,6 +309,7 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
             pc.charge(ch, DQMC_PH_LMUL);
         }
         tau_left = te;
+        if (alt) udv_copy(Pj(boundary ? (l + 1) / stab : M), left, n);   /* dqmc.c:704-706,767 */
         int ds;
         if (boundary) {
             udv_combine(n, left, Sj((l + 1) / stab), comb, w, s, flag);
@@ -327,6 +335,106 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
     return true;
 }
 
+/* Backward sweep of the alternating order, dqmc_sweep_backward
+ * (dqmc.c:815-950): slices L-1 .. 0 with B^-1 G B wraps (green.c:529-548);
+ * the suffix product is accumulated by rmul and stored as the next forward
+ * sweep's suffix stack; at a boundary G comes from the forward sweep's
+ * prefix and this suffix (green_from_boundary_factors, green.c:308-341). */
+__device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDev &md, int kflags,
+                                             Smem &s, int *flag, uint64_t *rng,
+                                             unsigned long long *att, unsigned long long *acc,
+                                             double *slot_scr)
+{
+    const int n = ch->n, L = ch->L, stab = ch->stab, M = ch->M, kb = ch->kb;
+    const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
+    const Scr w = chain_scr(ch);
+    double *G = ch->G, *Gn = ch->w[3], *tmp = ch->w[4], *tmp2 = ch->w[5];
+    const double v0 = md.expv[0], v1 = md.expv[1];
+    auto Sj = [&](int j) { return udv_at(ch->S + (size_t)j * usz, n); };
+    auto Pj = [&](int j) { return udv_at(ch->P + (size_t)j * usz, n); };
+    Udv left = udv_at(ch->left, n), comb = udv_at(ch->comb, n);
+    PhaseClock pc;
+    pc.mark();
+    if (!ch->pvalid) {
+        /* green_stack_build_prefix (green.c:228-250) */
+        udv_identity(Pj(0), n);
+        for (int j = 1; j <= M; ++j) {
+            const int b0 = (j - 1) * stab, b1 = min(j * stab, L);
+            bblock(n, b0, b1 - b0, ch->field, md.expK, v0, v1, ch->bcache + (j - 1) * nn, tmp,
+                   tmp2, s);
+            udv_copy(Pj(j), Pj(j - 1), n);
+            udv_lmul(n, Pj(j), ch->bcache + (j - 1) * nn, nullptr, nullptr, 0.0, 0.0, w, s,
+                     flag);
+            if (*flag) return false;
+        }
+    }
+    udv_identity(left, n);
+    udv_identity(Sj(M), n);
+    pc.charge(ch, DQMC_PH_STACK);
+    auto back_wrap = [&](int l) {
+        wrap_green_back(n, G, tmp, md.expK, md.expKinv, ch->field + (size_t)l * n, v0, v1,
+                        md.expvinv[0], md.expvinv[1], s);
+        pc.charge(ch, DQMC_PH_WRAP);
+    };
+    auto rebuild = [&](int tau, Udv u, bool boundary, int j) {
+        if (kflags & KF_SDRIFT) {
+            const int ds = green_scratch(ch, md, tau, Gn, slot_scr, s, flag);
+            if (*flag || ds == 0) return false;
+            const double d = max_diff(n, G, Gn, s);
+            if (threadIdx.x == 0) {
+                ch->sdrift_count++;
+                ch->sdrift_sum += d;
+                if (d > ch->sdrift_max || ch->sdrift_count == 1) {
+                    ch->sdrift_max = d;
+                    ch->sdrift_max_tau = tau;
+                    ch->sdrift_max_sweep = ch->sweeps;
+                }
+            }
+            pc.charge(ch, DQMC_PH_SDRIFT);
+        }
+        const int b1 = min(tau + stab, L);
+        bblock(n, tau, b1 - tau, ch->field, md.expK, v0, v1, ch->bcache + j * nn, tmp, tmp2, s);
+        pc.charge(ch, DQMC_PH_BBLOCK);
+        udv_rmul(n, u, ch->bcache + j * nn, w, s, flag);
+        if (*flag) return false;
+        pc.charge(ch, DQMC_PH_LMUL);
+        int ds;
+        if (boundary) {
+            udv_copy(Sj(j), u, n);
+            udv_combine(n, Pj(j), u, comb, w, s, flag);
+            if (*flag) return false;
+            pc.charge(ch, DQMC_PH_COMBINE);
+            ds = udv_green(n, comb, Gn, w, s, flag);
+        } else {
+            ds = udv_green(n, u, Gn, w, s, flag);
+        }
+        pc.charge(ch, DQMC_PH_GREEN);
+        if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
+        __syncthreads();
+        if (*flag) return false;
+        const double d = adopt_green(n, G, Gn, s);
+        if (threadIdx.x == 0) {
+            ch->drift_count++;
+            ch->drift_sum += d;
+            if (d > ch->drift_max || ch->drift_count == 1) ch->drift_max = d;
+            ch->sign = 1.0;
+        }
+        pc.charge(ch, DQMC_PH_ADOPT);
+        return true;
+    };
+    back_wrap(L - 1);
+    for (int l = L - 1; l >= 0; --l) {
+        signed char *fl = ch->field + (size_t)l * n;
+        for (int i0 = 0; i0 < n; i0 += kb)
+            site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs, ch->Ys,
+                       s, ch, pc);
+        if (l == 0) break;
+        if (l % stab == 0 && !rebuild(l, left, true, l / stab)) return false;
+        back_wrap(l - 1);
+    }
+    return rebuild(0, left, false, 0);
+}
+
 __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps)
 {
@@ -349,7 +457,9 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
             ch->meas_attempts = ch->attempts;
         }
         __syncthreads();
-        const bool ok = sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
+        const bool back = ch->alt && ch->dir;
+        const bool ok = back ? sweep_body_back(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr)
+                             : sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int i = 0; i < 4; ++i) ch->rng[i] = rng[i];
@@ -358,10 +468,17 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
             if (ok && !flag) {
                 ch->sweeps++;
                 ch->bvalid = 1;
+                if (ch->alt) {   /* dqmc.c:806-810, 943-946 */
+                    ch->dir = back ? 0 : 1;
+                    ch->pvalid = back ? 0 : 1;
+                    ch->svalid = back ? 1 : 0;
+                }
             } else {
                 ch->status = flag ? flag : DQMC_ST_NONFINITE;
                 ch->sign = 0.0;
                 ch->bvalid = 0;
+                ch->pvalid = 0;
+                ch->svalid = 0;
             }
         }
         __syncthreads();
@@ -385,6 +502,9 @@ __global__ void __launch_bounds__(NT, DQMC_MINB) k_init(DqmcChainDev *chains, co
         ch->status = flag ? flag : (ds == 0 ? DQMC_ST_DETSIGN : 0);
         ch->sign = ch->status ? 0.0 : 1.0;
         ch->bvalid = 0;
+        ch->dir = 0;
+        ch->pvalid = 0;
+        ch->svalid = 0;
     }
 }
 

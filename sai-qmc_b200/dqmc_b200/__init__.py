@@ -19,6 +19,7 @@ PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.environ.get("DQMC_B200_LIB") or os.path.join(PKG, "libdqmc_b200.so")
 
 PREC_FP64, PREC_MIXED = 0, 1
+SWEEP_FORWARD, SWEEP_ALTERNATING = 0, 1
 DRIFT_STAB, DRIFT_SCRATCH = 1, 2
 BIN_FIELDS = ["sum_sign_Ehub", "sum_sign_Egc", "sum_sign_Eph", "sum_sign_N",
               "sum_sign_D", "sum_sign", "count", "accepted", "attempts"]
@@ -34,7 +35,7 @@ _bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
 class Desc(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int),
                 ("delay_rank", C.c_int), ("drift", C.c_int),
-                ("ctas_per_sm", C.c_int), ("reserved", C.c_int * 7)]
+                ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class Counters(C.Structure):
@@ -189,12 +190,13 @@ class Engine:
     """A batch of chains on one GPU (the C ABI's dqmc_engine)."""
 
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
-                 drift=DRIFT_STAB, ctas_per_sm=0):
+                 drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
         d.device, d.precision, d.delay_rank, d.drift = device, precision, delay_rank, drift
         d.ctas_per_sm = ctas_per_sm
+        d.sweep_order = sweep_order
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
             raise DqmcError(L.dqmc_last_error().decode())

@@ -205,12 +205,11 @@ int dqmc_host_run(const char *input)
         fprintf(stderr, "ERROR: udv_centered_file requires green_rebuild=centered\n");
         goto out;
     }
-    if (strcmp(p.sweep_order, "forward") || strcmp(p.green_rebuild, "combine") ||
-        p.udv_scale_file[0] || p.udv_centered_file[0]) {
+    if (strcmp(p.green_rebuild, "combine") || p.udv_scale_file[0] || p.udv_centered_file[0]) {
         fprintf(stderr,
-                "ERROR: the GPU engine implements sweep_order=forward with "
-                "green_rebuild=combine; sweep_order=%s green_rebuild=%s%s is not available\n",
-                p.sweep_order, p.green_rebuild,
+                "ERROR: the GPU engine implements green_rebuild=combine; "
+                "green_rebuild=%s%s is not available\n",
+                p.green_rebuild,
                 (p.udv_scale_file[0] || p.udv_centered_file[0]) ? " with UDV diagnostics" : "");
         goto out;
     }
@@ -383,6 +382,8 @@ int dqmc_host_run(const char *input)
         d.device = p.gpu_device;
         d.precision = !strcmp(p.precision, "mixed") ? DQMC_PREC_MIXED : DQMC_PREC_FP64;
         d.delay_rank = p.delay_rank;
+        d.sweep_order = !strcmp(p.sweep_order, "alternating") ? DQMC_SWEEP_ALTERNATING
+                                                              : DQMC_SWEEP_FORWARD;
         d.drift = DQMC_DRIFT_STAB | (p.stab_drift_file[0] ? DQMC_DRIFT_SCRATCH : 0);
         eng = dqmc_engine_create(&d);
         if (!eng) {

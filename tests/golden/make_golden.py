@@ -5,13 +5,18 @@ default /root/reference): ``python tests/golden/make_golden.py``.  It
 builds oracle/_ref (oracle/build.py), drives the reference engine through
 oracle/ref_shim.c and writes small .npz files next to this script.  The
 reference's own UDV fixtures (tests/fixtures/udv_phase6a_*.txt, read here as
-data) are re-packed into udv_fixture.npz.  The GPU box never needs the
+data) are re-packed into udv_fixture.npz.  ``--only-alternating`` writes
+just the sweep_order=alternating fixtures (*_alt.npz).  The GPU box never needs the
 reference: tests read only the .npz files.
 """
 from __future__ import annotations
 
+import io
 import os
+import subprocess
 import sys
+
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
 
 import numpy as np
 
@@ -32,6 +37,17 @@ CASES = [
     ("sq6_b2", LAT_SQUARE, 6, 6, 6.0, 0.1, 20, 8, 3, 3, "af"),
     ("sq8_b4", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 2, "af"),
 ]
+
+# sweep_order=alternating (forward sweeps storing the prefix stack, backward
+# sweeps with B^-1 G B wraps rebuilding the suffix stack): 4 sweeps each
+# (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps)
+ALT_CASES = [
+    ("chain4_alt", LAT_CHAIN, 4, 1, 4.0, 0.1, 20, 8, 1, 4),
+    ("sq4_b4_alt", LAT_SQUARE, 4, 4, 4.0, 0.1, 40, 10, 7, 4),
+    ("sq6_b2_alt", LAT_SQUARE, 6, 6, 6.0, 0.1, 20, 8, 3, 4),
+    ("sq8_b4_alt", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 4),
+]
+HEADLINE_ALT = dict(Lx=16, U=4.0, dtau=0.1, L=80, stab=8, base_seed=11, chains=2, sweeps=4)
 
 # the headline lattice: 16x16 U=4 dtau=0.1 beta=8 stab=8, chains seeded as
 # the benchmark's replicas (replica_seed(11, 0, r)); fields and drift only
@@ -72,9 +88,85 @@ def udv_fixture(out):
                         max_logD=float(rec["max_logD"][0]))
 
 
+def alternating(R):
+    for (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps) in ALT_CASES:
+        ch = R.chain(kind, Lx, Ly, U, dtau, L, stab, seed, drift=True, alternating=True)
+        st0 = ch.state()
+        fields, Gs, cnt = [], [], []
+        for _ in range(sweeps):
+            ch.sweep(1)
+            st = ch.state()
+            fields.append(st["field"])
+            Gs.append(st["Gu"])
+            cnt.append([st["attempts"], st["accepted"], st["sweeps"], st["status"]])
+        np.savez_compressed(
+            os.path.join(HERE, f"{name}.npz"),
+            params=np.array([kind, Lx, Ly, L, stab, seed, sweeps], dtype=np.int64),
+            U=U, dtau=dtau, field0=st0["field"], G0=st0["Gu"], fields=np.array(fields),
+            Gs=np.array(Gs), counters=np.array(cnt, dtype=np.int64), drift=R.drift(ch),
+            rng_end=st["rng"])
+        ch.free()
+    h = HEADLINE_ALT
+    seeds, fields, drifts, cnts, Gend = [], [], [], [], []
+    for r in range(h["chains"]):
+        seed = R.replica_seed(h["base_seed"], 0, r)
+        ch = R.chain(LAT_SQUARE, h["Lx"], h["Lx"], h["U"], h["dtau"], h["L"], h["stab"], seed,
+                     drift=True, alternating=True)
+        fr = []
+        for _ in range(h["sweeps"]):
+            ch.sweep(1)
+            fr.append(ch.state()["field"])
+        st = ch.state()
+        seeds.append(seed)
+        fields.append(fr)
+        drifts.append(R.drift(ch))
+        cnts.append([st["attempts"], st["accepted"]])
+        Gend.append(st["Gu"][:8, :8])
+        ch.free()
+    # the same chains with 4 BLAS threads (a rounding variant of the same
+    # reference): chain 0's first backward sweep meets an acceptance decision
+    # at the rounding level (slice 17, site 236), which the variant takes the
+    # other way; both trajectories are the reference's
+    var = subprocess.run([sys.executable, __file__, "--headline-alt-fields"], check=True,
+                         capture_output=True, env=dict(os.environ, OPENBLAS_NUM_THREADS="4"))
+    variant = np.load(io.BytesIO(var.stdout))
+    np.savez_compressed(os.path.join(HERE, "sq16_b8_alt.npz"), fields_t4=variant,
+                        params=np.array([h["Lx"], h["L"], h["stab"], h["sweeps"]]),
+                        U=h["U"], dtau=h["dtau"], seeds=np.array(seeds, dtype=np.uint64),
+                        fields=np.array(fields), drift=np.array(drifts),
+                        counters=np.array(cnts, dtype=np.int64), G_corner=np.array(Gend))
+
+
+def headline_alt_fields():
+    """Fields of the alternating headline chains, written as .npy to stdout."""
+    R = Reference()
+    h = HEADLINE_ALT
+    out = []
+    for r in range(h["chains"]):
+        seed = R.replica_seed(h["base_seed"], 0, r)
+        ch = R.chain(LAT_SQUARE, h["Lx"], h["Lx"], h["U"], h["dtau"], h["L"], h["stab"], seed,
+                     drift=True, alternating=True)
+        fr = []
+        for _ in range(h["sweeps"]):
+            ch.sweep(1)
+            fr.append(ch.state()["field"])
+        out.append(fr)
+        ch.free()
+    buf = io.BytesIO()
+    np.save(buf, np.array(out))
+    sys.stdout.buffer.write(buf.getvalue())
+
+
 def main():
+    if "--headline-alt-fields" in sys.argv:
+        headline_alt_fields()
+        return
     obuild.build_ref()
     R = Reference()
+    if "--only-alternating" in sys.argv:
+        alternating(R)
+        print("wrote alternating fixtures")
+        return
     # RNG streams and replica seeds (rng.c:17-37, replica.c:17-34)
     seeds = np.array([1, 7, 11, 12345, 2**63 + 5], dtype=np.uint64)
     draws = np.stack([R.rng(int(s), 16) for s in seeds])
@@ -138,6 +230,7 @@ def main():
                         fields=np.array(fields), drift=np.array(drifts),
                         counters=np.array(cnts, dtype=np.int64), G_corner=np.array(Gend))
     udv_fixture(os.path.join(HERE, "udv_fixture.npz"))
+    alternating(R)
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

@@ -36,8 +36,8 @@ EXE = os.path.join(PKG, "dqmc_gpu")
 REF_EXE = os.path.join(ROOT, "oracle", "_ref", "dqmc")
 
 
-def run(exe, d):
-    (d / "input.txt").write_text(INPUT)
+def run(exe, d, extra=""):
+    (d / "input.txt").write_text(INPUT + extra)
     r = subprocess.run([exe, "input.txt"], cwd=d, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     return r
@@ -117,3 +117,20 @@ def test_cli_rejects_like_reference(tmp_path):
     (tmp_path / "input.txt").write_text("beta_list=0.55\ndtau=0.1\nnmeas=4\nnbin=2\n")
     r = subprocess.run([EXE, "input.txt"], cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 1 and "not a multiple of dtau" in r.stderr
+
+
+def test_cli_alternating_matches_reference(tmp_path):
+    """sweep_order=alternating through the whole program: the same rows as
+    the reference program's alternating run."""
+    if not os.path.exists(REF_EXE):
+        pytest.skip("reference program not built here")
+    extra = "sweep_order=alternating\nstab=4\n"
+    gdir, rdir = tmp_path / "gpu", tmp_path / "ref"
+    gdir.mkdir()
+    rdir.mkdir()
+    run(EXE, gdir, extra)
+    run(REF_EXE, rdir, extra)
+    for name in ("observables.dat", "szz.dat", "sperp.dat", "consistency.dat"):
+        a, b = table(gdir / name), table(rdir / name)
+        assert a.shape == b.shape
+        np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-9, err_msg=name)
