@@ -247,10 +247,11 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------ GPU arm
-def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB, ctas_per_sm=0):
+def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB, ctas_per_sm=0,
+                sweep_order=0):
     T, bp = dq.square_lattice(LX, LX)
     eng = dq.Engine(device=device, precision=precision, delay_rank=delay_rank,
-                    ctas_per_sm=ctas_per_sm)
+                    ctas_per_sm=ctas_per_sm, sweep_order=sweep_order)
     m = eng.add_model(T, bp, U, DTAU, LX, LX, szz="af", sperp="af")
     for r in range(chains):
         eng.add_chain(m, L_SLICES, STAB, dq_replica_seed(SEED, 0, seed0 + r))
@@ -352,6 +353,26 @@ def precision_compare(dq, chains, args, precision, value):
             "same_seed_check": {"chains": 4, "sweeps": 2, "identical_flips": same,
                                 "max_abs_dG_after_sweeps": dg,
                                 "stabilization_drift_max": drift}}
+
+
+def alternating_order(dq, chains, args, precision, value):
+    """The same workload in sweep_order=alternating (forward sweeps carrying
+    the prefix stack, backward sweeps rebuilding the suffix stack): timed
+    over an even number of sweeps after the same warm-up."""
+    e = make_engine(dq, chains, 0, precision, sweep_order=dq.SWEEP_ALTERNATING)
+    e.prepare(1)
+    for _ in range(max(4, args.warmup + (args.warmup & 1))):
+        e.sweep(1)
+    e.sync()
+    k = max(2, args.steps + (args.steps & 1))
+    e.mark(0)
+    e.sweep(k)
+    e.mark(1)
+    ms = e.elapsed_ms() / k
+    e.close()
+    v = chains * N_SITES * L_SLICES / (ms * 1e-3)
+    return {"value": v, "unit": UNIT, "ms_per_sweep": ms, "over_forward": v / value,
+            "sweeps": k}
 
 
 def run_gpu_arm(args):
@@ -459,6 +480,7 @@ def run_gpu_arm(args):
         }
         if world == 1 and not args.no_compare:
             line["precision_compare"] = precision_compare(dq, chains, args, precision, value)
+            line["alternating_order"] = alternating_order(dq, chains, args, precision, value)
         if not args.no_single_chain and world == 1:
             e1 = make_engine(dq, 1, 0, precision)
             e1.prepare(1)
