@@ -32,6 +32,13 @@ enum { DQMC_PREC_FP64 = 0, DQMC_PREC_MIXED = 1 };
  * alternating forward / backward sweeps carrying the prefix and suffix UDV
  * stacks between them (src/dqmc.c:609-963). */
 enum { DQMC_SWEEP_FORWARD = 0, DQMC_SWEEP_ALTERNATING = 1 };
+/* G rebuild at a stabilization boundary (GreenRebuildMode, src/green.h):
+ * COMBINE = one UDV from the two factors, then (1+UDT)^-1 (udv_combine +
+ * udv_inv_one_plus_work, src/linalg.c:796-1115); TWO_SIDED = (1+LR)^-1 from
+ * the two factors directly (udv_inv_one_plus_two_sided_work,
+ * src/linalg.c:1117-1389).  CENTERED (the reference's recentred-D variant of
+ * two-sided) is the same computation here: D is always held as log D. */
+enum { DQMC_REBUILD_COMBINE = 0, DQMC_REBUILD_TWO_SIDED = 1, DQMC_REBUILD_CENTERED = 2 };
 enum { DQMC_DRIFT_STAB = 1, DQMC_DRIFT_SCRATCH = 2 };
 
 /* Per-bin scalar layout returned by dqmc_read_bins (src/replica.h:6-16). */
@@ -59,7 +66,8 @@ typedef struct {
     int ctas_per_sm; /* sweep kernel residency: 0 = auto (two chains per SM
                         when there are more chains than SMs), 1 or 2      */
     int sweep_order; /* DQMC_SWEEP_*                                        */
-    int reserved[6];
+    int green_rebuild; /* DQMC_REBUILD_*                                    */
+    int reserved[5];
 } dqmc_engine_desc;
 
 typedef struct {
@@ -179,6 +187,16 @@ int dqmc_wrap_green(dqmc_engine *e, int chain, int l, double *G);
  * the reference). */
 int dqmc_udv_green(int device, int n, const double *U, const double *D,
                    const double *T, double *G, int *det_sign);
+
+/* G = (1 + U_L D_L T_L U_R D_R T_R)^-1 and the sign of its determinant from
+ * two caller UDV factors (host arrays, column-major n x n; D values signed;
+ * the factors are scaled by exp(off_L), exp(off_R) as the reference's
+ * log_offset; T_R must be unit upper triangular), by the two-sided
+ * reconstruction.  Replaces udv_inv_one_plus_two_sided_work
+ * (src/linalg.c:1117-1389).  n <= DQMC_MAX_N. */
+int dqmc_udv_green2(int device, int n, const double *UL, const double *DL, const double *TL,
+                    double off_L, const double *UR, const double *DR, const double *TR,
+                    double off_R, double *G, int *det_sign);
 
 /* Host helper: out = exp(scale * A) for symmetric A (la_expm_sym,
  * src/linalg.c:319-346). */

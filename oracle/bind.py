@@ -209,7 +209,7 @@ class Reference:
                                       C.c_int, C.c_int, C.c_ulonglong,
                                       C.c_void_p, C.c_int]
         lib.ref_chain_new_mode.restype = C.c_void_p
-        lib.ref_chain_new_mode.argtypes = lib.ref_chain_new.argtypes + [C.c_int]
+        lib.ref_chain_new_mode.argtypes = lib.ref_chain_new.argtypes + [C.c_int, C.c_int]
         lib.ref_chain_sweep.argtypes = [C.c_void_p, C.c_int]
         lib.ref_chain_state.argtypes = [C.c_void_p, _dp, _dp, _bp, _up,
                                         C.c_void_p, C.c_void_p, _up]
@@ -232,14 +232,14 @@ class Reference:
         self.lib = lib
 
     def chain(self, kind, Lx, Ly, U, dtau, L, stab, seed, field=None,
-              pbc=1, t=-1.0, drift=False, alternating=False):
+              pbc=1, t=-1.0, drift=False, alternating=False, rebuild=0):
         n = Lx * (Ly if kind == LAT_SQUARE else 1)
         fp = None
         if field is not None:
             fa = np.ascontiguousarray(np.asarray(field, dtype=np.int8).ravel())
             fp = fa.ctypes.data_as(C.c_void_p)
         h = self.lib.ref_chain_new_mode(kind, Lx, Ly, pbc, t, U, dtau, L, stab,
-                                        seed, fp, int(drift), int(alternating))
+                                        seed, fp, int(drift), int(alternating), int(rebuild))
         ch = _Chain(self.lib, "ref_", h, n, L)
         ch.kind, ch.Lx, ch.Ly = kind, Lx, (Ly if kind == LAT_SQUARE else 1)
         return ch

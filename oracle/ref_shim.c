@@ -12,7 +12,7 @@
  *                      model_init (model.c:8-31), rng_seed (rng.c:17-22),
  *                      field_init (field.c:6-24), dqmc_init_modes
  *                      (dqmc.c:418-483)
- *   ref_chain_new_mode the same with sweep_order (forward / alternating)
+ *   ref_chain_new_mode the same with sweep_order and green_rebuild
  *   ref_chain_sweep    dqmc_sweep (dqmc.c:952-963)
  *   ref_chain_measure  measure_sample (measure.c:6-39) and
  *                      measure_szz_sperp_sample (structure_factor.c:328-400)
@@ -45,21 +45,24 @@ typedef struct {
 
 void *ref_chain_new_mode(int kind, int Lx, int Ly, int pbc, double t, double U,
                          double dtau, int L, int stab, unsigned long long seed,
-                         const signed char *field, int enable_drift, int sweep_mode);
+                         const signed char *field, int enable_drift, int sweep_mode,
+                         int rebuild_mode);
 
 void *ref_chain_new(int kind, int Lx, int Ly, int pbc, double t, double U,
                     double dtau, int L, int stab, unsigned long long seed,
                     const signed char *field, int enable_drift)
 {
     return ref_chain_new_mode(kind, Lx, Ly, pbc, t, U, dtau, L, stab, seed, field,
-                              enable_drift, 0);
+                              enable_drift, 0, 0);
 }
 
 /* As ref_chain_new with the reference's sweep order (DqmcSweepMode:
- * 0 forward, 1 alternating forward/backward, dqmc.h:45-48). */
+ * 0 forward, 1 alternating forward/backward, dqmc.h:45-48) and G rebuild
+ * (GreenRebuildMode: 0 combine, 1 two-sided, 2 centered, green.h). */
 void *ref_chain_new_mode(int kind, int Lx, int Ly, int pbc, double t, double U,
                          double dtau, int L, int stab, unsigned long long seed,
-                         const signed char *field, int enable_drift, int sweep_mode)
+                         const signed char *field, int enable_drift, int sweep_mode,
+                         int rebuild_mode)
 {
     RefChain *c = calloc(1, sizeof(RefChain));
     if (c == NULL) {
@@ -79,7 +82,9 @@ void *ref_chain_new_mode(int kind, int Lx, int Ly, int pbc, double t, double U,
     c->stab = stab;
     if (dqmc_init_modes(&c->D, &c->m, &c->f, &c->r, stab, NULL,
                         sweep_mode ? DQMC_SWEEP_ALTERNATING : DQMC_SWEEP_FORWARD,
-                        GREEN_REBUILD_COMBINE) != 0) {
+                        rebuild_mode == 1   ? GREEN_REBUILD_TWO_SIDED
+                        : rebuild_mode == 2 ? GREEN_REBUILD_CENTERED
+                                            : GREEN_REBUILD_COMBINE) != 0) {
         c->D.status = 1;
     }
     if (enable_drift) {

@@ -79,6 +79,7 @@ typedef struct {
      * backward) and whether the prefix stack P (after a forward sweep) or
      * the suffix stack S (after a backward sweep) carries over */
     int alt, dir, pvalid, svalid;
+    int rebuild;               /* 0: combine, 1: two-sided G at boundaries */
     double sign;
     unsigned long long attempts, accepted, sweeps;
     unsigned long long meas_accepted, meas_attempts;  /* counters at last measurement */
@@ -111,4 +112,6 @@ typedef struct {
 } DqmcChainDev;
 
 /* UDV slot: U (n*n) | T (n*n) | ell = log D (n) | detU (1) | pad (1)        */
-#define DQMC_UDV_SIZE(n) (2 * (size_t)(n) * (n) + (size_t)(n) + 2)
+/* UDV slot: U (n x n) | T (n x n) | log D (n) | sign det U | pad | column
+ * permutation of an rmul factor, T = R_unit P^T (n, stored as doubles) */
+#define DQMC_UDV_SIZE(n) (2 * (size_t)(n) * (n) + 2 * (size_t)(n) + 2)

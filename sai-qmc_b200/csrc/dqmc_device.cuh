@@ -1379,13 +1379,13 @@ __device__ __forceinline__ void qr_apply_qt(int n, const double *A, const double
 
 /* ------------------------------------------------------------------ UDV */
 struct Udv {
-    double *U, *T, *ell, *det;
+    double *U, *T, *ell, *det, *perm;
 };
 
 __device__ __forceinline__ Udv udv_at(double *base, int n)
 {
     const size_t nn = (size_t)n * n;
-    return Udv{base, base + nn, base + 2 * nn, base + 2 * nn + n};
+    return Udv{base, base + nn, base + 2 * nn, base + 2 * nn + n, base + 2 * nn + n + 2};
 }
 
 __device__ void udv_identity(Udv u, int n)
@@ -1395,7 +1395,10 @@ __device__ void udv_identity(Udv u, int n)
         u.U[e] = v;
         u.T[e] = v;
     }
-    for (int i = threadIdx.x; i < n; i += NT) u.ell[i] = 0.0;
+    for (int i = threadIdx.x; i < n; i += NT) {
+        u.ell[i] = 0.0;
+        u.perm[i] = (double)i;
+    }
     if (threadIdx.x == 0) *u.det = 1.0;
     __syncthreads();
 }
@@ -1406,7 +1409,10 @@ __device__ void udv_copy(Udv d, Udv s, int n)
     double *dU = d.U, *dT = d.T;
     ew_batched(n * n, [=](int e) { return sU[e]; }, [=](int e, double x) { dU[e] = x; });
     ew_batched(n * n, [=](int e) { return sT[e]; }, [=](int e, double x) { dT[e] = x; });
-    for (int i = threadIdx.x; i < n; i += NT) d.ell[i] = s.ell[i];
+    for (int i = threadIdx.x; i < n; i += NT) {
+        d.ell[i] = s.ell[i];
+        d.perm[i] = s.perm[i];
+    }
     if (threadIdx.x == 0) *d.det = *s.det;
     __syncthreads();
 }
@@ -1519,7 +1525,10 @@ __device__ __noinline__ void udv_rmul(int n, Udv u, const double *B, Scr w, Smem
                 uT[i + (size_t)perm[r] * n] = r >= i ? x / rd[i] : 0.0;
             });
     }
-    for (int i = threadIdx.x; i < n; i += NT) u.ell[i] = s.vB[i];
+    for (int i = threadIdx.x; i < n; i += NT) {
+        u.ell[i] = s.vB[i];
+        u.perm[i] = (double)s.perm[i];
+    }
     __syncthreads();
     if (threadIdx.x == 0) *u.det = *u.det * ((nt & 1) ? -1.0 : 1.0) * sg;
     __syncthreads();
@@ -1632,6 +1641,108 @@ __device__ __noinline__ int udv_green(int n, Udv u, double *G, Scr w, Smem &s, i
     if (bad != 0.0) raise_flag(flag, DQMC_ST_NONFINITE);
     const double dU = *u.det;
     return (int)(dU * ((nt & 1) ? -1.0 : 1.0) * sg);
+}
+
+/* Y[i, j] = sc[i] * U[j, i] (n x n): U^T row-scaled, read through shared
+ * memory 32 columns of U at a time when the shared-memory QR area exists. */
+__device__ void scaled_transpose(int n, const double *U, const double *sc, double *Y, Smem &s)
+{
+    if (s.q.cb >= 32) {
+        const int lds = n + 1;
+        double *S = s.q.X;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int nc = min(32, n - c0);
+            ew_batched(n * 32, [=](int e) {
+                const int j = e % n, c = e / n;
+                return c < nc ? U[j + (size_t)(c0 + c) * n] : 0.0;
+            }, [=](int e, double x) { S[(e % n) + (e / n) * lds] = x; });
+            __syncthreads();
+            for (int e = threadIdx.x; e < n * 32; e += NT) {
+                const int c = e & 31, j = e >> 5;
+                if (c < nc) Y[(c0 + c) + (size_t)j * n] = sc[c0 + c] * S[j + c * lds];
+            }
+            __syncthreads();
+        }
+    } else {
+        for (int e = threadIdx.x; e < n * n; e += NT) {
+            const int i = e % n, j = e / n;
+            Y[e] = sc[i] * U[j + (size_t)i * n];
+        }
+        __syncthreads();
+    }
+}
+
+/* G = (1 + L R)^{-1} for two UDV factors without forming their product
+ * (udv_inv_one_plus_two_sided_work, linalg.c:1117-1389; green_rebuild =
+ * two_sided | centered): with D = Db Ds (Db = max(D,1), Ds = min(D,1), all
+ * held as exp of the log scale, so every factor below is <= 1)
+ *     1 + U_L D_L T_L U_R D_R T_R = U_L Db_L H Db_R T_R,
+ *     H = Db_L^-1 U_L^T T_R^-1 Db_R^-1 + Ds_L (T_L U_R) Ds_R,
+ *     G = T_R^-1 Db_R^-1 H^-1 Db_L^-1 U_L^T,
+ * with T_R = R_unit P^T (the right factor is an rmul product), so T_R^-1 =
+ * P R_unit^-1.  H^-1 by a Householder QR solve.  Sign of det(1 + L R) =
+ * det U_L * det H.  X: one more n x n scratch. */
+__device__ __noinline__ int udv_green2(int n, Udv l, Udv r, double *G, double *X, Scr w, Smem &s,
+                                       int *flag)
+{
+    double *Ru = w.m2, *Tinv = w.m0, *A = w.m1;
+    const double *TR = r.T, *rp = r.perm;
+    /* R_unit = T_R P (column gather), R_unit^-1 by a unit-triangular solve */
+    ew_batched(n * n, [=](int e) {
+        const int i = e % n, c = e / n;
+        return TR[i + (size_t)rp[c] * n];
+    }, [=](int e, double x) { Ru[e] = x; });
+    for (int e = threadIdx.x; e < n * n; e += NT) Tinv[e] = (e % n == e / n) ? 1.0 : 0.0;
+    __syncthreads();
+    trsm_upper(n, Ru, Tinv, A, s);
+    /* T_R^-1 = P R_unit^-1: row r of R_unit^-1 is row perm[r] of T_R^-1 */
+    ew_batched(n * n, [=](int e) { return A[e]; }, [=](int e, double x) {
+        const int rr = e % n, c = e / n;
+        Tinv[(int)rp[rr] + (size_t)c * n] = x;
+    });
+    __syncthreads();
+    double *dbl = s.vA, *dsl = s.vB, *dsr = s.vC, *dbr = s.vD;
+    for (int i = threadIdx.x; i < n; i += NT) {
+        const double a = l.ell[i], b = r.ell[i];
+        dbl[i] = exp(-fmax(a, 0.0));
+        dsl[i] = exp(fmin(a, 0.0));
+        dbr[i] = exp(-fmax(b, 0.0));
+        dsr[i] = exp(fmin(b, 0.0));
+    }
+    __syncthreads();
+    const double *UL = l.U, *TL = l.T, *UR = r.U, *Ti = Tinv;
+    /* A = U_L^T T_R^-1, H (in Ru) = T_L U_R, then H <- scalings */
+    gemm_sq<false, true>(
+        n, n, n, [=](int i, int k) { return UL[k + (size_t)i * n]; },
+        [=](int k, int j) { return Ti[k + (size_t)j * n]; },
+        [=](int i, int j, double v) { A[i + (size_t)j * n] = v; }, s.gsm);
+    gemm_nn(n, n, n, TL, n, UR, n, [=](int i, int j, double v) { Ru[i + (size_t)j * n] = v; },
+            s.gsm);
+    {
+        const double *Ac = A;
+        double *H = Ru;
+        ew_batched(n * n, [=](int e) { return Ac[e]; }, [=](int e, double a) {
+            const int i = e % n, j = e / n;
+            H[e] = (dbl[i] * a) * dbr[j] + (dsl[i] * H[e]) * dsr[j];
+        });
+    }
+    __syncthreads();
+    /* right-hand side Db_L^-1 U_L^T, QR solve of H */
+    scaled_transpose(n, UL, dbl, A, s);
+    const int nt = qr_factor(n, Ru, w.tw, s, flag);
+    const int sg = qr_diag(n, Ru, s, flag);
+    qr_apply_qt(n, Ru, w.tw, A, n, s);
+    trsm_upper(n, Ru, A, X, s);
+    /* G = T_R^-1 (Db_R^-1 X) */
+    ew_batched(n * n, [=](int e) { return X[e]; }, [=](int e, double x) { X[e] = dbr[e % n] * x; });
+    __syncthreads();
+    gemm_nn(n, n, n, Tinv, n, X, n, [=](int i, int j, double v) { G[i + (size_t)j * n] = v; },
+            s.gsm);
+    double bad = 0.0;
+    for (int e = threadIdx.x; e < n * n; e += NT) bad += isfinite(G[e]) ? 0.0 : 1.0;
+    bad = block_reduce<false>(bad, s.red);
+    if (bad != 0.0) raise_flag(flag, DQMC_ST_NONFINITE);
+    return (int)(*l.det * ((nt & 1) ? -1.0 : 1.0) * sg);
 }
 
 /* ----------------------------------------------------- slice operations */

@@ -225,6 +225,10 @@ dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
                 d.sweep_order);
         return nullptr;
     }
+    if (d.green_rebuild < DQMC_REBUILD_COMBINE || d.green_rebuild > DQMC_REBUILD_CENTERED) {
+        set_err("green_rebuild %d is not a DQMC_REBUILD_* value", d.green_rebuild);
+        return nullptr;
+    }
     if (d.precision != DQMC_PREC_FP64 && d.precision != DQMC_PREC_MIXED) {
         set_err("precision %d is neither DQMC_PREC_FP64 nor DQMC_PREC_MIXED", d.precision);
         return nullptr;
@@ -535,6 +539,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         d.S = (double *)take((size_t)(c.M + 1) * usz * 8);
         if (alt) d.P = (double *)take((size_t)(c.M + 1) * usz * 8);
         d.alt = alt ? 1 : 0;
+        d.rebuild = e->desc.green_rebuild != DQMC_REBUILD_COMBINE ? 1 : 0;
         d.left = (double *)take(usz * 8);
         d.comb = (double *)take(usz * 8);
         d.scr = (double *)take(usz * 8);
@@ -910,6 +915,68 @@ int dqmc_udv_green(int device, int n, const double *U, const double *D, const do
     if (err == cudaSuccess) err = cudaMemcpy(det_sign, ddet, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(buf);
     if (err != cudaSuccess) return set_err("dqmc_udv_green: %s", cudaGetErrorString(err));
+    return 0;
+}
+
+/* caller factor -> engine slot: signs of D into U's columns, log|D| + off */
+static void host_udv_slot(int n, const double *U, const double *D, const double *T, double off,
+                          std::vector<double> &slot)
+{
+    const size_t nn = (size_t)n * n;
+    slot.assign(DQMC_UDV_SIZE(n), 0.0);
+    int dsign = host_det_sign(n, U);
+    for (int j = 0; j < n; ++j) {
+        const double sgn = D[j] < 0 ? -1.0 : 1.0;
+        if (D[j] < 0) dsign = -dsign;
+        for (int i = 0; i < n; ++i) slot[i + (size_t)j * n] = U[i + (size_t)j * n] * sgn;
+        slot[2 * nn + j] = std::log(std::fabs(D[j])) + off;
+        slot[2 * nn + n + 2 + j] = j;   /* identity column permutation */
+    }
+    std::memcpy(slot.data() + nn, T, nn * 8);
+    slot[2 * nn + n] = dsign;
+}
+
+int dqmc_udv_green2(int device, int n, const double *UL, const double *DL, const double *TL,
+                    double off_L, const double *UR, const double *DR, const double *TR,
+                    double off_R, double *G, int *det_sign)
+{
+    if (n <= 0 || n > DQMC_MAX_N || !UL || !DL || !TL || !UR || !DR || !TR || !G || !det_sign ||
+        !std::isfinite(off_L) || !std::isfinite(off_R))
+        return set_err("dqmc_udv_green2: bad arguments");
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i)
+            if (TR[i + (size_t)j * n] != (i == j ? 1.0 : 0.0))
+                return set_err("dqmc_udv_green2: T_R must be unit upper triangular");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err("dqmc_udv_green2: no CUDA device");
+    CU(cudaSetDevice(device));
+    const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
+    std::vector<double> ls, rs;
+    host_udv_slot(n, UL, DL, TL, off_L, ls);
+    host_udv_slot(n, UR, DR, TR, off_R, rs);
+    const size_t twsz = (size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB * DQMC_QNB;
+    char *buf = nullptr;
+    const size_t bytes = 2 * usz * 8 + (4 * nn + twsz) * 8 + nn * 8 + 64;
+    CU(cudaMalloc(&buf, bytes));
+    double *dl = (double *)buf, *dr = dl + usz, *ws = dr + usz;
+    double *dG = ws + 4 * nn + twsz;
+    int *ddet = (int *)(dG + nn);
+    cudaError_t err = cudaMemcpy(dl, ls.data(), usz * 8, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(dr, rs.data(), usz * 8, cudaMemcpyHostToDevice);
+    const size_t sm = dq::smem_bytes(n, 1);
+    if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(dq::k_udv_green2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sm);
+    if (err == cudaSuccess) {
+        dq::k_udv_green2<<<1, DQMC_NT, sm>>>(n, dl, dr, ws, dG, ddet);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    if (err == cudaSuccess) err = cudaMemcpy(G, dG, nn * 8, cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess) err = cudaMemcpy(det_sign, ddet, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (err != cudaSuccess) return set_err("dqmc_udv_green2: %s", cudaGetErrorString(err));
     return 0;
 }
 

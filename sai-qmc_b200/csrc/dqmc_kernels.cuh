@@ -311,7 +311,9 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         tau_left = te;
         if (alt) udv_copy(Pj(boundary ? (l + 1) / stab : M), left, n);   /* dqmc.c:704-706,767 */
         int ds;
-        if (boundary) {
+        if (boundary && ch->rebuild) {
+            ds = udv_green2(n, left, Sj((l + 1) / stab), Gn, tmp2, w, s, flag);
+        } else if (boundary) {
             udv_combine(n, left, Sj((l + 1) / stab), comb, w, s, flag);
             if (*flag) return false;
             pc.charge(ch, DQMC_PH_COMBINE);
@@ -401,10 +403,14 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
         int ds;
         if (boundary) {
             udv_copy(Sj(j), u, n);
-            udv_combine(n, Pj(j), u, comb, w, s, flag);
-            if (*flag) return false;
-            pc.charge(ch, DQMC_PH_COMBINE);
-            ds = udv_green(n, comb, Gn, w, s, flag);
+            if (ch->rebuild) {
+                ds = udv_green2(n, Pj(j), u, Gn, tmp2, w, s, flag);
+            } else {
+                udv_combine(n, Pj(j), u, comb, w, s, flag);
+                if (*flag) return false;
+                pc.charge(ch, DQMC_PH_COMBINE);
+                ds = udv_green(n, comb, Gn, w, s, flag);
+            }
         } else {
             ds = udv_green(n, u, Gn, w, s, flag);
         }
@@ -557,6 +563,22 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     const size_t nn = (size_t)n * n;
     Scr w{ws, ws + nn, ws + 2 * nn, ws + 3 * nn};
     const int ds = udv_green(n, udv_at(slot, n), G, w, s, &flag);
+    if (threadIdx.x == 0) *det = flag ? 0 : ds;
+}
+
+/* Two caller UDV slots -> G by the two-sided reconstruction (fixture
+ * parity).  ws: 4 n*n scratch + tw. */
+__global__ void __launch_bounds__(NT, DQMC_MINB)
+    k_udv_green2(int n, double *lslot, double *rslot, double *ws, double *G, int *det)
+{
+    extern __shared__ double smraw[];
+    __shared__ int flag;
+    if (threadIdx.x == 0) flag = 0;
+    __syncthreads();
+    Smem s = carve(smraw, n, 1);
+    const size_t nn = (size_t)n * n;
+    Scr w{ws, ws + nn, ws + 2 * nn, ws + 4 * nn};
+    const int ds = udv_green2(n, udv_at(lslot, n), udv_at(rslot, n), G, ws + 3 * nn, w, s, &flag);
     if (threadIdx.x == 0) *det = flag ? 0 : ds;
 }
 

@@ -20,6 +20,7 @@ LIB_PATH = os.environ.get("DQMC_B200_LIB") or os.path.join(PKG, "libdqmc_b200.so
 
 PREC_FP64, PREC_MIXED = 0, 1
 SWEEP_FORWARD, SWEEP_ALTERNATING = 0, 1
+REBUILD_COMBINE, REBUILD_TWO_SIDED, REBUILD_CENTERED = 0, 1, 2
 DRIFT_STAB, DRIFT_SCRATCH = 1, 2
 BIN_FIELDS = ["sum_sign_Ehub", "sum_sign_Egc", "sum_sign_Eph", "sum_sign_N",
               "sum_sign_D", "sum_sign", "count", "accepted", "attempts"]
@@ -35,7 +36,8 @@ _bp = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
 class Desc(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int),
                 ("delay_rank", C.c_int), ("drift", C.c_int),
-                ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("reserved", C.c_int * 6)]
+                ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("green_rebuild", C.c_int),
+                ("reserved", C.c_int * 5)]
 
 
 class Counters(C.Structure):
@@ -98,6 +100,8 @@ def lib():
     L.dqmc_wrap_green.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     L.dqmc_udv_green.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                  C.POINTER(C.c_int)]
+    L.dqmc_udv_green2.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp,
+                                  C.c_double, _dp, C.POINTER(C.c_int)]
     L.dqmc_expm_sym.argtypes = [C.c_int, _dp, C.c_double, _dp]
     L.dqmc_udv_green_noalloc.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                          C.POINTER(C.c_int)]
@@ -190,13 +194,15 @@ class Engine:
     """A batch of chains on one GPU (the C ABI's dqmc_engine)."""
 
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
-                 drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD):
+                 drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD,
+                 green_rebuild=REBUILD_COMBINE):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
         d.device, d.precision, d.delay_rank, d.drift = device, precision, delay_rank, drift
         d.ctas_per_sm = ctas_per_sm
         d.sweep_order = sweep_order
+        d.green_rebuild = green_rebuild
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
             raise DqmcError(L.dqmc_last_error().decode())
@@ -343,6 +349,19 @@ def udv_green(U, D, T, device=0):
     _check(lib().dqmc_udv_green(device, n, _cm(U),
                                 np.ascontiguousarray(D, dtype=np.float64), _cm(T), g,
                                 C.byref(ds)), "udv_green")
+    return _from_cm(g, n), ds.value
+
+
+def udv_green2(UL, DL, TL, off_L, UR, DR, TR, off_R, device=0):
+    """G = (1 + L R)^{-1} from two UDV factors scaled by exp(off) (T_R unit
+    upper triangular), two-sided reconstruction (dqmc_udv_green2)."""
+    n = UL.shape[0]
+    g = np.zeros(n * n)
+    ds = C.c_int()
+    _check(lib().dqmc_udv_green2(device, n, _cm(UL), np.ascontiguousarray(DL, dtype=np.float64),
+                                 _cm(TL), float(off_L), _cm(UR),
+                                 np.ascontiguousarray(DR, dtype=np.float64), _cm(TR),
+                                 float(off_R), g, C.byref(ds)), "udv_green2")
     return _from_cm(g, n), ds.value
 
 

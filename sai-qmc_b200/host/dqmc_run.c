@@ -205,12 +205,9 @@ int dqmc_host_run(const char *input)
         fprintf(stderr, "ERROR: udv_centered_file requires green_rebuild=centered\n");
         goto out;
     }
-    if (strcmp(p.green_rebuild, "combine") || p.udv_scale_file[0] || p.udv_centered_file[0]) {
-        fprintf(stderr,
-                "ERROR: the GPU engine implements green_rebuild=combine; "
-                "green_rebuild=%s%s is not available\n",
-                p.green_rebuild,
-                (p.udv_scale_file[0] || p.udv_centered_file[0]) ? " with UDV diagnostics" : "");
+    if (p.udv_scale_file[0] || p.udv_centered_file[0]) {
+        fprintf(stderr, "ERROR: the GPU engine does not write udv_scale_file / "
+                        "udv_centered_file diagnostics\n");
         goto out;
     }
     if (p.stab_drift_file[0]) {
@@ -384,6 +381,9 @@ int dqmc_host_run(const char *input)
         d.delay_rank = p.delay_rank;
         d.sweep_order = !strcmp(p.sweep_order, "alternating") ? DQMC_SWEEP_ALTERNATING
                                                               : DQMC_SWEEP_FORWARD;
+        d.green_rebuild = !strcmp(p.green_rebuild, "two_sided")  ? DQMC_REBUILD_TWO_SIDED
+                          : !strcmp(p.green_rebuild, "centered") ? DQMC_REBUILD_CENTERED
+                                                                 : DQMC_REBUILD_COMBINE;
         d.drift = DQMC_DRIFT_STAB | (p.stab_drift_file[0] ? DQMC_DRIFT_SCRATCH : 0);
         eng = dqmc_engine_create(&d);
         if (!eng) {

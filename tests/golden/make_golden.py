@@ -6,7 +6,8 @@ builds oracle/_ref (oracle/build.py), drives the reference engine through
 oracle/ref_shim.c and writes small .npz files next to this script.  The
 reference's own UDV fixtures (tests/fixtures/udv_phase6a_*.txt, read here as
 data) are re-packed into udv_fixture.npz.  ``--only-alternating`` writes
-just the sweep_order=alternating fixtures (*_alt.npz).  The GPU box never needs the
+just the sweep_order=alternating fixtures (*_alt.npz), ``--only-rebuild``
+the green_rebuild=two_sided/centered ones.  The GPU box never needs the
 reference: tests read only the .npz files.
 """
 from __future__ import annotations
@@ -46,6 +47,14 @@ ALT_CASES = [
     ("sq4_b4_alt", LAT_SQUARE, 4, 4, 4.0, 0.1, 40, 10, 7, 4),
     ("sq6_b2_alt", LAT_SQUARE, 6, 6, 6.0, 0.1, 20, 8, 3, 4),
     ("sq8_b4_alt", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 4),
+]
+# green_rebuild=two_sided / centered (G from the two boundary factors):
+# (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, alternating, rebuild)
+REBUILD_CASES = [
+    ("sq4_b4_2s", LAT_SQUARE, 4, 4, 4.0, 0.1, 40, 10, 7, 3, False, 1),
+    ("sq8_b4_2s", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 3, False, 1),
+    ("chain4_ctr", LAT_CHAIN, 4, 1, 4.0, 0.1, 20, 8, 1, 3, False, 2),
+    ("sq6_b2_2s_alt", LAT_SQUARE, 6, 6, 6.0, 0.1, 20, 8, 3, 4, True, 1),
 ]
 HEADLINE_ALT = dict(Lx=16, U=4.0, dtau=0.1, L=80, stab=8, base_seed=11, chains=2, sweeps=4)
 
@@ -137,6 +146,45 @@ def alternating(R):
                         counters=np.array(cnts, dtype=np.int64), G_corner=np.array(Gend))
 
 
+def rebuild_modes(R):
+    for (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, alt, rb) in REBUILD_CASES:
+        ch = R.chain(kind, Lx, Ly, U, dtau, L, stab, seed, drift=True, alternating=alt,
+                     rebuild=rb)
+        st0 = ch.state()
+        fields, Gs, cnt = [], [], []
+        for _ in range(sweeps):
+            ch.sweep(1)
+            st = ch.state()
+            fields.append(st["field"])
+            Gs.append(st["Gu"])
+            cnt.append([st["attempts"], st["accepted"], st["sweeps"], st["status"]])
+        np.savez_compressed(
+            os.path.join(HERE, f"{name}.npz"),
+            params=np.array([kind, Lx, Ly, L, stab, seed, sweeps, int(alt), rb], dtype=np.int64),
+            U=U, dtau=dtau, field0=st0["field"], fields=np.array(fields), Gs=np.array(Gs),
+            counters=np.array(cnt, dtype=np.int64), drift=R.drift(ch), rng_end=st["rng"])
+        ch.free()
+    # the reference's two-sided fixture (tests/fixtures/udv_phase6a_two_sided_n4.txt)
+    tok = _read_tokens(os.path.join(REF, "tests", "fixtures", "udv_phase6a_two_sided_n4.txt"))
+    rec, key, vals = {}, None, []
+    for t in tok:
+        try:
+            vals.append(float(t))
+        except ValueError:
+            if key is not None:
+                rec[key] = vals
+            key, vals = t, []
+    rec[key] = vals
+    n = int(rec["n"][0])
+    cm = lambda v: np.array(v).reshape(n, n).T        # noqa: E731 (file is column-major)
+    np.savez_compressed(os.path.join(HERE, "udv_two_sided_fixture.npz"),
+                        UL=cm(rec["left_U"]), DL=np.array(rec["left_D"]), TL=cm(rec["left_T"]),
+                        off_L=rec["left_offset"][0], UR=cm(rec["right_U"]),
+                        DR=np.array(rec["right_D"]), TR=cm(rec["right_T"]),
+                        off_R=rec["right_offset"][0], G=cm(rec["G"]),
+                        det_sign=int(rec["det_sign"][0]))
+
+
 def headline_alt_fields():
     """Fields of the alternating headline chains, written as .npy to stdout."""
     R = Reference()
@@ -166,6 +214,10 @@ def main():
     if "--only-alternating" in sys.argv:
         alternating(R)
         print("wrote alternating fixtures")
+        return
+    if "--only-rebuild" in sys.argv:
+        rebuild_modes(R)
+        print("wrote green_rebuild fixtures")
         return
     # RNG streams and replica seeds (rng.c:17-37, replica.c:17-34)
     seeds = np.array([1, 7, 11, 12345, 2**63 + 5], dtype=np.uint64)
@@ -231,6 +283,7 @@ def main():
                         counters=np.array(cnts, dtype=np.int64), G_corner=np.array(Gend))
     udv_fixture(os.path.join(HERE, "udv_fixture.npz"))
     alternating(R)
+    rebuild_modes(R)
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 
