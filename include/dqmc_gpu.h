@@ -159,6 +159,15 @@ int dqmc_read_field(dqmc_engine *e, int chain, signed char *field);
 /* Replaces a chain's field and rebuilds its G from scratch. */
 int dqmc_write_field(dqmc_engine *e, int chain, const signed char *field);
 int dqmc_read_counters(dqmc_engine *e, int chain, dqmc_chain_counters *out);
+/* Overwrites a chain's G (n x n, column-major host array) without rebuilding
+ * it -- the reference's callers own D.Gu.g and its tests corrupt it to check
+ * the failure path (tests/test_dqmc.c); a G that is no longer finite stops
+ * the chain at its next stabilization point with DQMC_ST_NONFINITE. */
+int dqmc_write_green(dqmc_engine *e, int chain, const double *G);
+/* Sets a chain's xoshiro256** state (src/rng.h:6-8), e.g. to resume a run
+ * from a saved field (dqmc_write_field) and RNG state (read back with
+ * dqmc_read_counters).  No counterpart in the reference (no checkpointing). */
+int dqmc_write_rng(dqmc_engine *e, int chain, const uint64_t rng[4]);
 
 /* Copies back the bin accumulators: scalars nbin x DQMC_BIN_NFIELDS,
  * szz nbin x nq_zz, sperp nbin x nq_perp (either may be NULL). */

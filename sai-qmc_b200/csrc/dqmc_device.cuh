@@ -1590,12 +1590,14 @@ __device__ __noinline__ int udv_green(int n, Udv u, double *G, Scr w, Smem &s, i
     const double *U = u.U, *T = u.T, *ell = u.ell;
     double *X = w.m1, *Y = w.m0;
     double *dbi = s.vA, *dsm = s.vB;
+    double bad_ell = 0.0;
     for (int i = threadIdx.x; i < n; i += NT) {
         const double l = ell[i];
+        bad_ell += isfinite(l) ? 0.0 : 1.0;   /* fmax/fmin below would drop a NaN */
         dbi[i] = exp(-fmax(l, 0.0));
         dsm[i] = exp(fmin(l, 0.0));
     }
-    __syncthreads();
+    if (block_reduce<false>(bad_ell, s.red) != 0.0) raise_flag(flag, DQMC_ST_NONFINITE);
     if (s.q.cb >= 32) {
         /* U^T through shared memory, 32 columns of U at a time: columns of U
          * are read and rows of Y / X written in contiguous runs */
@@ -1702,14 +1704,16 @@ __device__ __noinline__ int udv_green2(int n, Udv l, Udv r, double *G, double *X
     });
     __syncthreads();
     double *dbl = s.vA, *dsl = s.vB, *dsr = s.vC, *dbr = s.vD;
+    double bad_ell = 0.0;
     for (int i = threadIdx.x; i < n; i += NT) {
         const double a = l.ell[i], b = r.ell[i];
+        bad_ell += (isfinite(a) && isfinite(b)) ? 0.0 : 1.0;
         dbl[i] = exp(-fmax(a, 0.0));
         dsl[i] = exp(fmin(a, 0.0));
         dbr[i] = exp(-fmax(b, 0.0));
         dsr[i] = exp(fmin(b, 0.0));
     }
-    __syncthreads();
+    if (block_reduce<false>(bad_ell, s.red) != 0.0) raise_flag(flag, DQMC_ST_NONFINITE);
     const double *UL = l.U, *TL = l.T, *UR = r.U, *Ti = Tinv;
     /* A = U_L^T T_R^-1, H (in Ru) = T_L U_R, then H <- scalings */
     gemm_sq<false, true>(

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstddef>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -740,6 +741,27 @@ int dqmc_write_field(dqmc_engine *e, int chain, const signed char *field)
     dq::k_init<<<1, DQMC_NT, e->smem, e->stream>>>(e->dchains + chain, e->dmodels);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(e->stream));
+    return 0;
+}
+
+int dqmc_write_green(dqmc_engine *e, int chain, const double *G)
+{
+    if (chain_ok(e, chain, "dqmc_write_green")) return 1;
+    if (!G) return set_err("dqmc_write_green: null G");
+    const DqmcChainDev &d = e->hdev[chain];
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(d.G, G, (size_t)d.n * d.n * 8, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int dqmc_write_rng(dqmc_engine *e, int chain, const uint64_t rng[4])
+{
+    if (chain_ok(e, chain, "dqmc_write_rng")) return 1;
+    if (!rng || (rng[0] | rng[1] | rng[2] | rng[3]) == 0)
+        return set_err("dqmc_write_rng: the all-zero xoshiro state is not valid");
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy((char *)(e->dchains + chain) + offsetof(DqmcChainDev, rng), rng,
+                  4 * sizeof(uint64_t), cudaMemcpyHostToDevice));
     return 0;
 }
 

@@ -174,7 +174,7 @@ __device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *
 /* max|G - Gn| and G <- Gn */
 __device__ double adopt_green(int n, double *G, const double *Gn, Smem &s)
 {
-    double mx = 0.0;
+    double mx = 0.0, bad = 0.0;
     for (int e0 = threadIdx.x; e0 < n * n; e0 += NT * 8) {
         double a[8], b[8];
 #pragma unroll
@@ -188,12 +188,17 @@ __device__ double adopt_green(int n, double *G, const double *Gn, Smem &s)
             const int e = e0 + u * NT;
             if (e < n * n) {
                 const double d = fabs(a[u] - b[u]);
-                mx = (d > mx || d != d) ? d : mx;
+                if (d <= 1.7976931348623157e308)
+                    mx = fmax(mx, d);
+                else
+                    bad += 1.0;             /* NaN or inf: counted, not maxed */
                 G[e] = b[u];
             }
         }
     }
-    return block_reduce<true>(mx, s.red);
+    mx = block_reduce<true>(mx, s.red);
+    bad = block_reduce<false>(bad, s.red);
+    return bad != 0.0 ? __longlong_as_double(0x7ff8000000000000LL) : mx;
 }
 
 __device__ double max_diff(int n, const double *A, const double *B, Smem &s)
@@ -326,6 +331,12 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         __syncthreads();
         if (*flag) return false;
         const double d = adopt_green(n, G, Gn, s);
+        /* a wrapped G that is not finite means the chain's state was lost
+         * since the last rebuild: stop the chain (sticky status) */
+        if (!(d == d) || isinf(d)) {
+            raise_flag(flag, DQMC_ST_NONFINITE);
+            return false;
+        }
         if (threadIdx.x == 0) {
             ch->drift_count++;
             ch->drift_sum += d;
@@ -419,6 +430,12 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
         __syncthreads();
         if (*flag) return false;
         const double d = adopt_green(n, G, Gn, s);
+        /* a wrapped G that is not finite means the chain's state was lost
+         * since the last rebuild: stop the chain (sticky status) */
+        if (!(d == d) || isinf(d)) {
+            raise_flag(flag, DQMC_ST_NONFINITE);
+            return false;
+        }
         if (threadIdx.x == 0) {
             ch->drift_count++;
             ch->drift_sum += d;

@@ -102,6 +102,8 @@ def lib():
                                  C.POINTER(C.c_int)]
     L.dqmc_udv_green2.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp,
                                   C.c_double, _dp, C.POINTER(C.c_int)]
+    L.dqmc_write_green.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.dqmc_write_rng.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_uint64)]
     L.dqmc_expm_sym.argtypes = [C.c_int, _dp, C.c_double, _dp]
     L.dqmc_udv_green_noalloc.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                          C.POINTER(C.c_int)]
@@ -270,6 +272,14 @@ class Engine:
     def write_field(self, c, field):
         f = np.ascontiguousarray(np.asarray(field, dtype=np.int8).ravel())
         _check(lib().dqmc_write_field(self.h, c, f), "write_field")
+
+    def write_green(self, c, G):
+        _check(lib().dqmc_write_green(self.h, c, _cm(np.asarray(G, dtype=np.float64))),
+               "write_green")
+
+    def write_rng(self, c, rng):
+        a = (C.c_uint64 * 4)(*[int(x) for x in rng])
+        _check(lib().dqmc_write_rng(self.h, c, a), "write_rng")
 
     def counters(self, c):
         out = Counters()
