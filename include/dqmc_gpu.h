@@ -40,6 +40,11 @@ enum { DQMC_SWEEP_FORWARD = 0, DQMC_SWEEP_ALTERNATING = 1 };
  * two-sided) is the same computation here: D is always held as log D. */
 enum { DQMC_REBUILD_COMBINE = 0, DQMC_REBUILD_TWO_SIDED = 1, DQMC_REBUILD_CENTERED = 2 };
 enum { DQMC_DRIFT_STAB = 1, DQMC_DRIFT_SCRATCH = 2 };
+/* Delayed-update flush grouping: AUTO pairs site blocks when n >= 128 (the
+ * G read-modify-write is bound by G traffic there), OFF flushes after every
+ * block of k sites (src/green.c:462-475 with k sites), ON always pairs.
+ * The proposals and their order are the same in all three. */
+enum { DQMC_PAIRS_AUTO = 0, DQMC_PAIRS_OFF = 1, DQMC_PAIRS_ON = 2 };
 
 /* Per-bin scalar layout returned by dqmc_read_bins (src/replica.h:6-16). */
 enum {
@@ -67,7 +72,9 @@ typedef struct {
                         when there are more chains than SMs), 1 or 2      */
     int sweep_order; /* DQMC_SWEEP_*                                        */
     int green_rebuild; /* DQMC_REBUILD_*                                    */
-    int reserved[5];
+    int flush_pairs; /* DQMC_PAIRS_*: stage two consecutive site blocks and
+                        update G once for both (rank <= 2k)               */
+    int reserved[4];
 } dqmc_engine_desc;
 
 typedef struct {

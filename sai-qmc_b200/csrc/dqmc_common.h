@@ -80,6 +80,7 @@ typedef struct {
      * the suffix stack S (after a backward sweep) carries over */
     int alt, dir, pvalid, svalid;
     int rebuild;               /* 0: combine, 1: two-sided G at boundaries */
+    int pair;                  /* flush G after every second site block   */
     double sign;
     unsigned long long attempts, accepted, sweeps;
     unsigned long long meas_accepted, meas_attempts;  /* counters at last measurement */
@@ -99,7 +100,7 @@ typedef struct {
     double *left, *comb, *scr; /* UDV slots (scr: rebuilds from scratch) */
     double *bcache;            /* M x n x n block products B(b_{j+1}, b_j) */
     double *w[6];              /* n x n scratch */
-    double *Zs, *Ys;           /* n x kb flush operands */
+    double *Zs, *Ys;           /* n x 2kb / 2kb x n flush operands (two blocks) */
     double *twall;             /* n x QNB compact-WY factors of the last QR */
     double *bins;              /* nbin x DQMC_BIN_FIELDS */
     double *bins_zz, *bins_perp;   /* nbin x nq */

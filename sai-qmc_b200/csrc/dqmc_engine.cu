@@ -226,6 +226,10 @@ dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
                 d.sweep_order);
         return nullptr;
     }
+    if (d.flush_pairs < DQMC_PAIRS_AUTO || d.flush_pairs > DQMC_PAIRS_ON) {
+        set_err("flush_pairs %d is not a DQMC_PAIRS_* value", d.flush_pairs);
+        return nullptr;
+    }
     if (d.green_rebuild < DQMC_REBUILD_COMBINE || d.green_rebuild > DQMC_REBUILD_CENTERED) {
         set_err("green_rebuild %d is not a DQMC_REBUILD_* value", d.green_rebuild);
         return nullptr;
@@ -498,7 +502,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += 3 * rup(usz * 8);                              /* left, comb, scr */
         off += rup((size_t)c.M * nn * 8);                     /* bcache */
         off += 6 * rup(nn * 8);                               /* w */
-        off += 2 * rup((size_t)n * c.kb * 8);                 /* Zs, Ys */
+        off += 2 * rup((size_t)n * 2 * c.kb * 8);             /* Zs, Ys */
         off += rup((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB * DQMC_QNB * 8);
         off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
@@ -541,13 +545,15 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         if (alt) d.P = (double *)take((size_t)(c.M + 1) * usz * 8);
         d.alt = alt ? 1 : 0;
         d.rebuild = e->desc.green_rebuild != DQMC_REBUILD_COMBINE ? 1 : 0;
+        d.pair = e->desc.flush_pairs == DQMC_PAIRS_ON ||
+                 (e->desc.flush_pairs == DQMC_PAIRS_AUTO && n >= 128);
         d.left = (double *)take(usz * 8);
         d.comb = (double *)take(usz * 8);
         d.scr = (double *)take(usz * 8);
         d.bcache = (double *)take((size_t)c.M * nn * 8);
         for (int i = 0; i < 6; ++i) d.w[i] = (double *)take(nn * 8);
-        d.Zs = (double *)take((size_t)n * c.kb * 8);
-        d.Ys = (double *)take((size_t)n * c.kb * 8);
+        d.Zs = (double *)take((size_t)n * 2 * c.kb * 8);
+        d.Ys = (double *)take((size_t)n * 2 * c.kb * 8);
         d.twall = (double *)take((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB *
                                  DQMC_QNB * 8);
         d.bins = (double *)take((size_t)e->nbin * DQMC_BIN_FIELDS * 8);

@@ -43,28 +43,70 @@ __device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
  * - sum_{q<p} V[:,q] C[i_p,q]; with the recorded entries this is
  * U (I - F Su) = E_A - G[:,A] and V (I + Sc) = G[A,:]^T (Su, Sc strictly
  * upper m x m), so U and V come from two unit-triangular inverses, and
- * G -= U F V^T is one rank-m GEMM (green_delay_flush, green.c:462-475). */
-__device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *G,
-                                        signed char *fl, const DqmcModelDev &md,
-                                        uint64_t *rng, unsigned long long *att,
-                                        unsigned long long *acc, double *Zs, double *Ys,
-                                        Smem &s, DqmcChainDev *ch, PhaseClock &pc)
+ * G -= U F V^T is one rank-m GEMM (green_delay_flush, green.c:462-475).
+ *
+ * Pairing: with mA > 0 the previous block's Zs_A, Ys_A (mA columns / rows)
+ * are staged but not yet subtracted from G, so this block works on
+ * G~ = G - Zs_A Ys_A: its proposals read G~[B,B], and by Woodbury
+ *   Zs_B = [(E_B - G[:,B]) Tu + Zs_A Qa] F,  Qa = Ys_A[:,B] Tu,
+ *   Ys_B = Tv^T G[B,:] - Pa Ys_A,            Pa = Tv^T Zs_A[B,:];
+ * one GEMM then subtracts both blocks (rank mA + m).  Returns the number
+ * of staged columns left for the next block (0 after a flush).
+ *
+ * Zs and Ys are formed one row / one column per thread (FP64 FMAs on the
+ * accepted columns / rows of G, coalesced across the CTA): no CTA-wide GEMM
+ * pipeline for these thin products. */
+__device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G,
+                                       signed char *fl, const DqmcModelDev &md,
+                                       uint64_t *rng, unsigned long long *att,
+                                       unsigned long long *acc, double *Zs, double *Ys,
+                                       int mA, bool flush, Smem &s, DqmcChainDev *ch,
+                                       PhaseClock &pc)
 {
     constexpr int KB = DQMC_MAX_KB;   /* 32: one lane per block column */
     constexpr int LD = KB + 1;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int LT = KB + 2;        /* even rows: 16-byte pair loads  */
+    static_assert(GEMM_SMEM >= 3 * KB * LT && GEMM_SMEM % 2 == 0, "site-block staging");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double *Rrow = s.g0;              /* [q*LD + b] = G~_q[a_q, b]      */
     double *Ccol = Rrow + KB * LD;    /* [q*LD + c] = G~_q[c, a_q]      */
     double *Tu = Ccol + KB * LD;      /* (I - F Su)^-1, row-major [q*LD+p] */
     double *Tv = Tu + KB * LD;        /* (I + Sc)^-1                     */
     double *facs = Tv + KB * LD;      /* fac_q                           */
-    int *alist = s.iscr;
+    /* GEMM staging area, idle until the final flush: the staged block's
+     * entries at this block ZA[a][k] = Zs_A[i0+a, k], YA[k][b] = Ys_A[k,
+     * i0+b] (row length LD), later -Pa^T and Qa (row length LT); TvP. */
+    double *ZA = s.gsm, *YA = s.gsm + KB * LT, *TvP = s.gsm + 2 * KB * LT;
+    double *TuP = Rrow;               /* Tu with row length LT, after the inverses */
+    int *alist = s.iscr;              /* accepted block positions, in order */
+    const int ldy = 2 * kb;
+    if (mA > 0) {
+        for (int e = tid; e < KB * KB; e += NT) {
+            const int a = e % KB, k = e / KB;
+            if (k < mA) ZA[a * LD + k] = a < kbs ? Zs[(i0 + a) + (size_t)k * n] : 0.0;
+            const int k2 = e % KB, b = e / KB;
+            if (k2 < mA) YA[k2 * LD + b] = b < kbs ? Ys[k2 + (size_t)(i0 + b) * ldy] : 0.0;
+        }
+        __syncthreads();
+        /* G~[B,B] = G[B,B] - ZA YA, row-major in the Tu area */
+        for (int e = tid; e < KB * KB; e += NT) {
+            const int c = e % KB, b = e / KB;
+            if (c < kbs && b < kbs) {
+                double v = G[(i0 + c) + (size_t)(i0 + b) * n];
+                for (int k = 0; k < mA; ++k) v = fma(-ZA[c * LD + k], YA[k * LD + b], v);
+                Tu[c * LD + b] = v;
+            }
+        }
+        __syncthreads();
+    }
     if (warp == 0) {
         double col[KB];
         const bool mine = lane < kbs;
 #pragma unroll
         for (int c = 0; c < KB; ++c)
-            col[c] = (mine && c < kbs) ? G[(i0 + c) + (size_t)(i0 + lane) * n] : 0.0;
+            col[c] = (mine && c < kbs) ? (mA > 0 ? Tu[c * LD + lane]
+                                                 : G[(i0 + c) + (size_t)(i0 + lane) * n])
+                                       : 0.0;
         int fvl = mine ? (int)fl[i0 + lane] : 1;
         const double Nu0 = md.Nup[0], Nu1 = md.Nup[1], Nd0 = md.Ndn[0], Nd1 = md.Ndn[1];
         uint64_t r4[4] = {0, 0, 0, 0};
@@ -122,53 +164,160 @@ __device__ __noinline__ void site_block(int n, int kb, int kbs, int i0, double *
     __syncthreads();
     pc.charge(ch, DQMC_PH_PROPOSE);
     const int m = s.iscr[2 * DQMC_MAX_KB];
-    if (m == 0) return;
+    if (m == 0) {
+        if (!flush || mA == 0) return mA;
+        gemm_nn_rmw(
+            n, n, mA, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
+            [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
+        pc.charge(ch, DQMC_PH_FLUSH);
+        return 0;
+    }
     /* Tu = (I - F Su)^-1 (warp 0), Tv = (I + Sc)^-1 (warp 1); lane q owns
      * row q.  Su[r][p] = V[i_p, r] = Rrow[r][a_p], Sc[r][p] = C[i_p, r] =
-     * -fac_r Ccol[r][a_p], both for r < p. */
+     * -fac_r Ccol[r][a_p], both for r < p.  Column p of row q is
+     * delta_qp + sum_{r<p} (T[q][r] fac_r) S[r][a_p], summed in increasing
+     * r; rolled loops over shared memory keep the code small and the
+     * register count low. */
     if (warp < 2) {
-        /* right-looking: once xr[r] is final its contribution goes to every
-         * later p, so each of the m steps is a row of independent FMAs */
         const double *Src = (warp == 0) ? Rrow : Ccol;
-        const int q = lane;
-        int ap[KB];
-        double xr[KB];
-#pragma unroll
-        for (int p = 0; p < KB; ++p) {
-            ap[p] = p < m ? alist[p] : 0;
-            xr[p] = (p == q) ? 1.0 : 0.0;
-        }
-#pragma unroll
-        for (int r = 0; r < KB - 1; ++r) {
-            if (r + 1 < m) {
-                const double c = xr[r] * facs[r];
-                const double *row = Src + r * LD;
-#pragma unroll
-                for (int p = r + 1; p < KB; ++p)
-                    if (p < m) xr[p] = fma(c, row[ap[p]], xr[p]);
-            }
-        }
         double *T = (warp == 0) ? Tu : Tv;
-#pragma unroll
-        for (int p = 0; p < KB; ++p)
-            if (p < m) T[q * LD + p] = xr[p];
+        const int q = lane;
+        for (int p = 0; p < m; ++p) {
+            const double *sp = Src + alist[p];
+            double x = (p == q) ? 1.0 : 0.0;
+            for (int r = 0; r < p; ++r) x = fma(T[q * LD + r] * facs[r], sp[r * LD], x);
+            T[q * LD + p] = x;
+        }
     }
     __syncthreads();
-    /* Zs = (E_A - G[:,A]) Tu F  (n x m),  Ys = Tv^T G[A,:]  (m x n) */
-    gemm_sq<true, true>(
-        n, m, m, [=](int i, int k) { return G[i + (size_t)(i0 + alist[k]) * n]; },
-        [=](int k, int j) { return Tu[k * LD + j]; },
-        [=](int i, int j, double v) { Zs[i + (size_t)j * n] = v * facs[j]; }, s.gsm,
-        [=](int i, int k, double x) { return (i == i0 + alist[k] ? 1.0 : 0.0) - x; });
-    gemm<TMmaWide, false, true>(
-        m, n, m, [=](int i, int k) { return Tv[k * LD + i]; },
-        [=](int k, int j) { return G[(i0 + alist[k]) + (size_t)j * n]; },
-        [=](int i, int j, double v) { Ys[i + (size_t)j * kb] = v; }, s.gsm);
-    /* G -= Zs Ys */
+    /* TuP, TvP: Tu, Tv with even rows, zero outside m x m.  With a staged
+     * block: Qa[k][p] = sum_q YA[k][a_q] Tu[q][p] and -Pa^T[k][p] =
+     * -sum_q ZA[a_q][k] Tv[q][p] (k < mA), kept in registers until every
+     * thread has read ZA and YA. */
+    constexpr int KR = KB * KB / NT;
+    double qa[KR], pa[KR];
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+        const int e = tid + r * NT, q = e / KB, p = e % KB;
+        const bool on = q < m && p < m;
+        TuP[q * LT + p] = on ? Tu[q * LD + p] : 0.0;
+        TvP[q * LT + p] = on ? Tv[q * LD + p] : 0.0;
+        double x = 0.0, y = 0.0;
+        if (mA > 0 && q < mA && p < m) {   /* here q indexes the staged k */
+            for (int t = 0; t < m; ++t) {
+                const int at = alist[t];
+                x = fma(YA[q * LD + at], Tu[t * LD + p], x);
+                y = fma(ZA[at * LD + q], Tv[t * LD + p], y);
+            }
+        }
+        qa[r] = x;
+        pa[r] = -y;
+    }
+    if (mA > 0) {
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < KR; ++r) {
+            const int e = tid + r * NT, k = e / KB, p = e % KB;
+            YA[k * LT + p] = qa[r];
+            ZA[k * LT + p] = pa[r];
+        }
+    }
+    __syncthreads();
+    pc.charge(ch, DQMC_PH_FLUSH);
+    /* Zs_B rows and Ys_B columns, after the mA staged ones */
+    const double *Qa = YA, *PaT = ZA;
+    double *ZsB = Zs + (size_t)mA * n;
+    double *YsB = Ys + mA;
+    for (int i = tid; i < n; i += NT) {
+        double x[KB];
+#pragma unroll
+        for (int q = 0; q < KB; ++q) {
+            const int c = i0 + alist[q];
+            x[q] = q < m ? (i == c ? 1.0 : 0.0) - G[i + (size_t)c * n] : 0.0;
+        }
+        for (int p0 = 0; p0 < m; p0 += 8) {
+            double z[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) z[u] = 0.0;
+#pragma unroll
+            for (int q0 = 0; q0 < KB; q0 += 8) {
+                if (q0 < m) {
+#pragma unroll
+                    for (int q = q0; q < q0 + 8; ++q) {
+#pragma unroll
+                        for (int u = 0; u < 8; u += 2) {
+                            const double2 t =
+                                *reinterpret_cast<const double2 *>(TuP + q * LT + p0 + u);
+                            z[u] = fma(x[q], t.x, z[u]);
+                            z[u + 1] = fma(x[q], t.y, z[u + 1]);
+                        }
+                    }
+                }
+            }
+            for (int k = 0; k < mA; ++k) {
+                const double zk = Zs[i + (size_t)k * n];
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                    const double2 t = *reinterpret_cast<const double2 *>(Qa + k * LT + p0 + u);
+                    z[u] = fma(zk, t.x, z[u]);
+                    z[u + 1] = fma(zk, t.y, z[u + 1]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = z[u] * facs[p0 + u];
+        }
+    }
+    for (int j = tid; j < n; j += NT) {
+        double y[KB];
+#pragma unroll
+        for (int q = 0; q < KB; ++q)
+            y[q] = q < m ? G[(i0 + alist[q]) + (size_t)j * n] : 0.0;
+        for (int p0 = 0; p0 < m; p0 += 8) {
+            double z[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) z[u] = 0.0;
+#pragma unroll
+            for (int q0 = 0; q0 < KB; q0 += 8) {
+                if (q0 < m) {
+#pragma unroll
+                    for (int q = q0; q < q0 + 8; ++q) {
+#pragma unroll
+                        for (int u = 0; u < 8; u += 2) {
+                            const double2 t =
+                                *reinterpret_cast<const double2 *>(TvP + q * LT + p0 + u);
+                            z[u] = fma(t.x, y[q], z[u]);
+                            z[u + 1] = fma(t.y, y[q], z[u + 1]);
+                        }
+                    }
+                }
+            }
+            for (int k = 0; k < mA; ++k) {
+                const double yk = Ys[k + (size_t)j * ldy];
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                    const double2 t = *reinterpret_cast<const double2 *>(PaT + k * LT + p0 + u);
+                    z[u] = fma(t.x, yk, z[u]);
+                    z[u + 1] = fma(t.y, yk, z[u + 1]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+        }
+    }
+    __syncthreads();
+    const int mt = mA + m;
+    if (!flush) {
+        pc.charge(ch, DQMC_PH_FLUSH);
+        return mt;
+    }
+    /* G -= Zs Ys, rank mA + m */
     gemm_nn_rmw(
-        n, n, m, Zs, n, Ys, kb, [=](int i, int j) { return G[i + (size_t)j * n]; },
+        n, n, mt, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
         [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
     pc.charge(ch, DQMC_PH_FLUSH);
+    return 0;
 }
 
 /* max|G - Gn| and G <- Gn */
@@ -272,9 +421,9 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
     int tau_left = 0;
     for (int l = 0; l < L; ++l) {
         signed char *fl = ch->field + (size_t)l * n;
-        for (int i0 = 0; i0 < n; i0 += kb)
-            site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs, ch->Ys,
-                       s, ch, pc);
+        for (int i0 = 0, mA = 0; i0 < n; i0 += kb)
+            mA = site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs,
+                            ch->Ys, mA, !ch->pair || mA > 0 || i0 + kb >= n, s, ch, pc);
 #if DQMC_MINB == 1
         if (kflags & KF_MIXED)
             wrap_green_mixed(n, G, tmp, md, fl, v0, v1, md.expvinv[0], md.expvinv[1], ch->mix,
@@ -448,9 +597,9 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     back_wrap(L - 1);
     for (int l = L - 1; l >= 0; --l) {
         signed char *fl = ch->field + (size_t)l * n;
-        for (int i0 = 0; i0 < n; i0 += kb)
-            site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs, ch->Ys,
-                       s, ch, pc);
+        for (int i0 = 0, mA = 0; i0 < n; i0 += kb)
+            mA = site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs,
+                            ch->Ys, mA, !ch->pair || mA > 0 || i0 + kb >= n, s, ch, pc);
         if (l == 0) break;
         if (l % stab == 0 && !rebuild(l, left, true, l / stab)) return false;
         back_wrap(l - 1);
@@ -461,7 +610,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
 __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     __shared__ uint64_t rng[4];
     __shared__ unsigned long long att, acc;
@@ -512,7 +661,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
 /* G from scratch at l0 = 0 for every chain (dqmc_init_modes, dqmc.c:466-483). */
 __global__ void __launch_bounds__(NT, DQMC_MINB) k_init(DqmcChainDev *chains, const DqmcModelDev *models)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     DqmcChainDev *ch = &chains[blockIdx.x];
     const DqmcModelDev &md = models[ch->model];
@@ -536,7 +685,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_scratch(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l0, double *out,
               int *det)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     DqmcChainDev *ch = &chains[c];
     const DqmcModelDev &md = models[ch->model];
@@ -551,7 +700,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_wrap(DqmcChainDev *chains, const DqmcModelDev *models, int c, int l, double *Gio,
            int kflags)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     DqmcChainDev *ch = &chains[c];
     const DqmcModelDev &md = models[ch->model];
     Smem s = carve(smraw, ch->n, ch->kb);
@@ -572,7 +721,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
 __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_udv_green(int n, double *slot, double *ws, double *G, int *det)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     if (threadIdx.x == 0) flag = 0;
     __syncthreads();
@@ -588,7 +737,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
 __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_udv_green2(int n, double *lslot, double *rslot, double *ws, double *G, int *det)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     if (threadIdx.x == 0) flag = 0;
     __syncthreads();
@@ -609,7 +758,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
 __global__ void __launch_bounds__(NT)
     k_measure(DqmcChainDev *chains, const DqmcModelDev *models, int bin)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ double red[40];
     DqmcChainDev *ch = &chains[blockIdx.x];
     if (ch->status) return;

@@ -57,7 +57,7 @@ namespace {
  * (U columns times sign(D), log|D|, T), then udv_green into G. */
 __global__ void __launch_bounds__(DQMC_NT, 1) k_udv_green_static(int n, double *base)
 {
-    extern __shared__ double smraw[];
+    extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     using namespace dqn;
     if (threadIdx.x == 0) flag = 0;

@@ -22,6 +22,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 SWEEP_FORWARD, SWEEP_ALTERNATING = 0, 1
 REBUILD_COMBINE, REBUILD_TWO_SIDED, REBUILD_CENTERED = 0, 1, 2
 DRIFT_STAB, DRIFT_SCRATCH = 1, 2
+PAIRS_AUTO, PAIRS_OFF, PAIRS_ON = 0, 1, 2
 BIN_FIELDS = ["sum_sign_Ehub", "sum_sign_Egc", "sum_sign_Eph", "sum_sign_N",
               "sum_sign_D", "sum_sign", "count", "accepted", "attempts"]
 NBIN_FIELDS = len(BIN_FIELDS)
@@ -37,7 +38,7 @@ class Desc(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int),
                 ("delay_rank", C.c_int), ("drift", C.c_int),
                 ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("green_rebuild", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("flush_pairs", C.c_int), ("reserved", C.c_int * 4)]
 
 
 class Counters(C.Structure):
@@ -197,7 +198,7 @@ class Engine:
 
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
                  drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD,
-                 green_rebuild=REBUILD_COMBINE):
+                 green_rebuild=REBUILD_COMBINE, flush_pairs=PAIRS_AUTO):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
@@ -205,6 +206,7 @@ class Engine:
         d.ctas_per_sm = ctas_per_sm
         d.sweep_order = sweep_order
         d.green_rebuild = green_rebuild
+        d.flush_pairs = flush_pairs
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
             raise DqmcError(L.dqmc_last_error().decode())

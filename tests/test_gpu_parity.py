@@ -23,9 +23,10 @@ def lattice(a):
     return T, bp, a["Lx"], a["Ly"]
 
 
-def engine_for(a, delay_rank=0, nbin=1, drift=dq.DRIFT_STAB, field=None, seeds=None):
+def engine_for(a, delay_rank=0, nbin=1, drift=dq.DRIFT_STAB, field=None, seeds=None,
+               flush_pairs=dq.PAIRS_AUTO):
     T, bp, Lx, Ly = lattice(a)
-    eng = dq.Engine(delay_rank=delay_rank, drift=drift)
+    eng = dq.Engine(delay_rank=delay_rank, drift=drift, flush_pairs=flush_pairs)
     m = eng.add_model(T, bp, a["U"], a["dtau"], Lx, Ly, szz=a["selector"],
                       sperp=a["selector"])
     for s in (seeds or [a["seed"]]):
@@ -57,9 +58,21 @@ def test_green_from_field(name):
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("kb", [0, 1, 5])
 def test_sweeps_match_reference(name, kb):
+    check_sweeps(name, kb, dq.PAIRS_AUTO)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("kb", [1, 5])
+def test_paired_flushes_match_reference(name, kb):
+    """Two site blocks staged per G update (rank <= 2k; the second block's
+    proposals read G - Z_A Y_A): same flips, counters, RNG, G and bins."""
+    check_sweeps(name, kb, dq.PAIRS_ON)
+
+
+def check_sweeps(name, kb, flush_pairs):
     g = golden(name)
     a = case_args(g)
-    eng = engine_for(a, delay_rank=kb, nbin=a["sweeps"])
+    eng = engine_for(a, delay_rank=kb, nbin=a["sweeps"], flush_pairs=flush_pairs)
     for s in range(a["sweeps"]):
         eng.sweep_measure(1, s)
         f = eng.field(0)
@@ -191,3 +204,26 @@ def test_headline_lattice_trajectory_matches_reference():
         assert (cnt["attempts"], cnt["accepted"]) == tuple(int(x) for x in g["counters"][c])
         assert cnt["scratch_drift_samples"] == int(g["drift"][c][0])
         assert cnt["scratch_drift_max"] < 10 * max(g["drift"][c][1], 1e-4)
+
+
+@pytest.mark.parametrize("sweep_order", [dq.SWEEP_FORWARD, dq.SWEEP_ALTERNATING])
+def test_paired_flushes_equal_single_on_large_lattice(sweep_order):
+    """n = 256 with 32-site blocks: pairs of blocks flushed together (the
+    default there) and every block flushed alone take the same decisions;
+    G agrees to rounding."""
+    T, bp = dq.square_lattice(16, 16)
+    out = []
+    for fp in (dq.PAIRS_OFF, dq.PAIRS_ON):
+        e = dq.Engine(flush_pairs=fp, sweep_order=sweep_order)
+        m = e.add_model(T, bp, 4.0, 0.1, 16, 16)
+        for sd in (11, 12):
+            e.add_chain(m, 40, 8, sd)
+        e.prepare(1)
+        e.sweep(2)
+        out.append([(e.field(c), e.green(c), e.counters(c)) for c in range(2)])
+        e.close()
+    for (f0, g0, c0), (f1, g1, c1) in zip(*out):
+        np.testing.assert_array_equal(f0, f1)
+        assert (c0["attempts"], c0["accepted"]) == (c1["attempts"], c1["accepted"])
+        assert np.max(np.abs(g0 - g1)) < 1e-9
+        assert c1["status"] == 0 and c1["drift_max"] < 1e-6
