@@ -175,18 +175,27 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
     /* Tu = (I - F Su)^-1 (warp 0), Tv = (I + Sc)^-1 (warp 1); lane q owns
      * row q.  Su[r][p] = V[i_p, r] = Rrow[r][a_p], Sc[r][p] = C[i_p, r] =
      * -fac_r Ccol[r][a_p], both for r < p.  Column p of row q is
-     * delta_qp + sum_{r<p} (T[q][r] fac_r) S[r][a_p], summed in increasing
-     * r; rolled loops over shared memory keep the code small and the
-     * register count low. */
+     * delta_qp + sum_{r<p} (T[q][r] fac_r) S[r][a_p]; rolled loops over
+     * shared memory keep the code small and the register count low. */
     if (warp < 2) {
         const double *Src = (warp == 0) ? Rrow : Ccol;
         double *T = (warp == 0) ? Tu : Tv;
         const int q = lane;
         for (int p = 0; p < m; ++p) {
             const double *sp = Src + alist[p];
-            double x = (p == q) ? 1.0 : 0.0;
-            for (int r = 0; r < p; ++r) x = fma(T[q * LD + r] * facs[r], sp[r * LD], x);
-            T[q * LD + p] = x;
+            const double *tq = T + q * LD;
+            /* four interleaved partial sums (r mod 4) to overlap the FP64
+             * latency, combined in a fixed order */
+            double x0 = (p == q) ? 1.0 : 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+            int r = 0;
+            for (; r + 4 <= p; r += 4) {
+                x0 = fma(tq[r] * facs[r], sp[r * LD], x0);
+                x1 = fma(tq[r + 1] * facs[r + 1], sp[(r + 1) * LD], x1);
+                x2 = fma(tq[r + 2] * facs[r + 2], sp[(r + 2) * LD], x2);
+                x3 = fma(tq[r + 3] * facs[r + 3], sp[(r + 3) * LD], x3);
+            }
+            for (; r < p; ++r) x0 = fma(tq[r] * facs[r], sp[r * LD], x0);
+            T[q * LD + p] = (x0 + x1) + (x2 + x3);
         }
     }
     __syncthreads();
@@ -195,39 +204,51 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
      * -sum_q ZA[a_q][k] Tv[q][p] (k < mA), kept in registers until every
      * thread has read ZA and YA. */
     constexpr int KR = KB * KB / NT;
-    double qa[KR], pa[KR];
+    static_assert(KR * NT == KB * KB, "block split");
 #pragma unroll
     for (int r = 0; r < KR; ++r) {
         const int e = tid + r * NT, q = e / KB, p = e % KB;
         const bool on = q < m && p < m;
         TuP[q * LT + p] = on ? Tu[q * LD + p] : 0.0;
         TvP[q * LT + p] = on ? Tv[q * LD + p] : 0.0;
-        double x = 0.0, y = 0.0;
-        if (mA > 0 && q < mA && p < m) {   /* here q indexes the staged k */
-            for (int t = 0; t < m; ++t) {
-                const int at = alist[t];
-                x = fma(YA[q * LD + at], Tu[t * LD + p], x);
-                y = fma(ZA[at * LD + q], Tv[t * LD + p], y);
-            }
-        }
-        qa[r] = x;
-        pa[r] = -y;
     }
     if (mA > 0) {
+        /* element r of this thread: staged index k = (tid + r NT) / KB
+         * (uniform across a warp), column p = lane; the KR sums interleave */
+        double qa[KR], pa[KR];
+#pragma unroll
+        for (int r = 0; r < KR; ++r) qa[r] = pa[r] = 0.0;
+        if (lane < m) {
+            for (int t = 0; t < m; ++t) {
+                const int at = alist[t];
+                const double tu = Tu[t * LD + lane], tv = Tv[t * LD + lane];
+#pragma unroll
+                for (int r = 0; r < KR; ++r) {
+                    const int k = (tid + r * NT) / KB;
+                    qa[r] = fma(YA[k * LD + at], tu, qa[r]);
+                    pa[r] = fma(ZA[at * LD + k], tv, pa[r]);
+                }
+            }
+        }
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < KR; ++r) {
-            const int e = tid + r * NT, k = e / KB, p = e % KB;
-            YA[k * LT + p] = qa[r];
-            ZA[k * LT + p] = pa[r];
+            const int k = (tid + r * NT) / KB;
+            const bool on = k < mA;
+            YA[k * LT + lane] = on ? qa[r] : 0.0;
+            ZA[k * LT + lane] = on ? -pa[r] : 0.0;
         }
     }
     __syncthreads();
     pc.charge(ch, DQMC_PH_FLUSH);
-    /* Zs_B rows and Ys_B columns, after the mA staged ones */
+    /* Zs_B rows and Ys_B columns, after the mA staged ones.  Pass 1: the
+     * G part, (E_B - G[:,B]) Tu and Tv^T G[B,:]; pass 2 (staged block):
+     * + Zs_A Qa and - Pa Ys_A, the staged operands of a row / column loaded
+     * as one batch; F scales Zs_B once, at the end. */
     const double *Qa = YA, *PaT = ZA;
     double *ZsB = Zs + (size_t)mA * n;
     double *YsB = Ys + mA;
+    const bool two = mA > 0;
     for (int i = tid; i < n; i += NT) {
         double x[KB];
 #pragma unroll
@@ -254,18 +275,9 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
                     }
                 }
             }
-            for (int k = 0; k < mA; ++k) {
-                const double zk = Zs[i + (size_t)k * n];
-#pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    const double2 t = *reinterpret_cast<const double2 *>(Qa + k * LT + p0 + u);
-                    z[u] = fma(zk, t.x, z[u]);
-                    z[u + 1] = fma(zk, t.y, z[u + 1]);
-                }
-            }
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-                if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = z[u] * facs[p0 + u];
+                if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = two ? z[u] : z[u] * facs[p0 + u];
         }
     }
     for (int j = tid; j < n; j += NT) {
@@ -292,18 +304,70 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
                     }
                 }
             }
-            for (int k = 0; k < mA; ++k) {
-                const double yk = Ys[k + (size_t)j * ldy];
-#pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    const double2 t = *reinterpret_cast<const double2 *>(PaT + k * LT + p0 + u);
-                    z[u] = fma(t.x, yk, z[u]);
-                    z[u + 1] = fma(t.y, yk, z[u + 1]);
-                }
-            }
 #pragma unroll
             for (int u = 0; u < 8; ++u)
                 if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+        }
+    }
+    if (two) {
+        /* each thread re-reads only what it wrote in pass 1 */
+        for (int i = tid; i < n; i += NT) {
+            double za[KB];
+#pragma unroll
+            for (int k = 0; k < KB; ++k) za[k] = k < mA ? Zs[i + (size_t)k * n] : 0.0;
+            for (int p0 = 0; p0 < m; p0 += 8) {
+                double z[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    z[u] = p0 + u < m ? ZsB[i + (size_t)(p0 + u) * n] : 0.0;
+#pragma unroll
+                for (int k0 = 0; k0 < KB; k0 += 8) {
+                    if (k0 < mA) {
+#pragma unroll
+                        for (int k = k0; k < k0 + 8; ++k) {
+#pragma unroll
+                            for (int u = 0; u < 8; u += 2) {
+                                const double2 t =
+                                    *reinterpret_cast<const double2 *>(Qa + k * LT + p0 + u);
+                                z[u] = fma(za[k], t.x, z[u]);
+                                z[u + 1] = fma(za[k], t.y, z[u + 1]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = z[u] * facs[p0 + u];
+            }
+        }
+        for (int j = tid; j < n; j += NT) {
+            double ya[KB];
+#pragma unroll
+            for (int k = 0; k < KB; ++k) ya[k] = k < mA ? Ys[k + (size_t)j * ldy] : 0.0;
+            for (int p0 = 0; p0 < m; p0 += 8) {
+                double z[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    z[u] = p0 + u < m ? YsB[(p0 + u) + (size_t)j * ldy] : 0.0;
+#pragma unroll
+                for (int k0 = 0; k0 < KB; k0 += 8) {
+                    if (k0 < mA) {
+#pragma unroll
+                        for (int k = k0; k < k0 + 8; ++k) {
+#pragma unroll
+                            for (int u = 0; u < 8; u += 2) {
+                                const double2 t =
+                                    *reinterpret_cast<const double2 *>(PaT + k * LT + p0 + u);
+                                z[u] = fma(t.x, ya[k], z[u]);
+                                z[u + 1] = fma(t.y, ya[k], z[u + 1]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+            }
         }
     }
     __syncthreads();
