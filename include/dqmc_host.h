@@ -20,6 +20,7 @@ extern "C" {
 #endif
 
 #define DQMC_MAX_BETA 64
+#define DQMC_MAX_GPUS 16
 
 /* Params of src/io.h:4-38 plus the engine's own keys. */
 typedef struct {
@@ -51,6 +52,9 @@ typedef struct {
     int delay_rank;       /* delay_rank=k, site-block size (0 = default) */
     char precision[16];   /* precision=fp64|mixed                        */
     int gpu_device;       /* gpu_device=ordinal                          */
+    int gpu_devices[DQMC_MAX_GPUS];  /* gpu_devices=0,1,...: replicas of each
+                                        beta split over these devices      */
+    int ngpu;             /* entries in gpu_devices (0: gpu_device alone) */
 } DqmcParams;
 
 /* params_read (src/io.c:156-418): 0 ok, 1 error (message on stderr). */
@@ -81,6 +85,19 @@ void dqmc_spin_plan_free(DqmcSpinPlan *plan);
 unsigned long long dqmc_replica_seed(unsigned long long base, int beta_index,
                                      int replica_id);
 void dqmc_jackknife(const double *x, int N, double *mean, double *err);
+
+/* Replica ownership across devices or ranks, as the reference's MPI runner
+ * splits the nrep replicas of each beta (src/replica_mpi.c:13-89): rank r
+ * owns the contiguous range [first, first + count), the first nrep % nranks
+ * ranks one replica more.  rank_for_replica returns the owner (-1 if out of
+ * range); gather_layout fills per-rank element counts and displacements of
+ * a replica-major (replica, bin, item) gather, 0 ok, 1 on bad arguments or
+ * int overflow. */
+void dqmc_replica_rank_range(int nrep, int nranks, int rank, int *first_replica,
+                             int *local_nrep);
+int dqmc_replica_rank_for_replica(int nrep, int nranks, int replica_id);
+int dqmc_replica_gather_layout(int nrep, int nbin, int nranks, int item_width,
+                               int *recvcounts, int *displs);
 
 /* replica_bin_values (src/replica.c:88-120) on one bin of
  * dqmc_read_bins' scalar layout; out = {Ehub, Egc, Eph, N, D, sign}. */

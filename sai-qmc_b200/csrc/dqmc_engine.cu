@@ -715,6 +715,8 @@ static int chain_ok(dqmc_engine *e, int chain, const char *who)
 {
     if (check_prepared(e, who)) return 1;
     if (chain < 0 || chain >= (int)e->chains.size()) return set_err("%s: bad chain %d", who, chain);
+    /* engines on different devices may be driven from one host thread */
+    if (cudaSetDevice(e->desc.device) != cudaSuccess) return set_err("%s: cudaSetDevice", who);
     return 0;
 }
 

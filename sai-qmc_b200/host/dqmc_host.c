@@ -4,8 +4,8 @@
  * reference's main() (SAI-QMC src/main.c:603-2099) with one batched GPU
  * engine: every (beta, replica) chain of the input advances together.
  * Formats and validation messages follow the reference so that outputs are
- * interchangeable; engine-specific keys are delay_rank, precision and
- * gpu_device.
+ * interchangeable; engine-specific keys are delay_rank, precision,
+ * gpu_device and gpu_devices.
  */
 #define _XOPEN_SOURCE 700
 #include "dqmc_host.h"
@@ -246,6 +246,18 @@ int dqmc_params_read(DqmcParams *p, const char *path)
         } else if (!strcmp(key, "gpu_device")) {
             if (parse_int(val, &p->gpu_device) || p->gpu_device < 0)
                 FAIL("ERROR: gpu_device must be a non-negative integer (got %s)\n", val);
+        } else if (!strcmp(key, "gpu_devices")) {
+            p->ngpu = 0;
+            char *tok = strtok(val, ",");
+            if (!tok) FAIL("ERROR: gpu_devices must list non-negative device ordinals\n");
+            while (tok) {
+                if (p->ngpu >= DQMC_MAX_GPUS)
+                    FAIL("ERROR: gpu_devices has too many entries (max %d)\n", DQMC_MAX_GPUS);
+                if (parse_int(tok, &p->gpu_devices[p->ngpu]) || p->gpu_devices[p->ngpu] < 0)
+                    FAIL("ERROR: gpu_devices must list non-negative device ordinals\n");
+                p->ngpu++;
+                tok = strtok(NULL, ",");
+            }
         } else {
             FAIL("ERROR: unknown key %s\n", key);
         }
@@ -527,6 +539,49 @@ int dqmc_spin_plan(DqmcSpinPlan *plan, const DqmcLattice *L, const char *sel)
 fail:
     dqmc_spin_plan_free(plan);
     return 1;
+}
+
+/* ------------------------------------------------- replica ownership */
+void dqmc_replica_rank_range(int nrep, int nranks, int rank, int *first_replica,
+                             int *local_nrep)
+{
+    int first = 0, count = 0;
+    if (nrep >= 0 && nranks > 0 && rank >= 0 && rank < nranks) {
+        const int base = nrep / nranks, rem = nrep % nranks;
+        count = base + (rank < rem);
+        first = rank * base + (rank < rem ? rank : rem);
+    }
+    if (first_replica) *first_replica = first;
+    if (local_nrep) *local_nrep = count;
+}
+
+int dqmc_replica_rank_for_replica(int nrep, int nranks, int replica_id)
+{
+    if (nrep <= 0 || nranks <= 0 || replica_id < 0 || replica_id >= nrep) return -1;
+    for (int r = 0; r < nranks; r++) {
+        int first, count;
+        dqmc_replica_rank_range(nrep, nranks, r, &first, &count);
+        if (replica_id >= first && replica_id < first + count) return r;
+    }
+    return -1;
+}
+
+int dqmc_replica_gather_layout(int nrep, int nbin, int nranks, int item_width,
+                               int *recvcounts, int *displs)
+{
+    if (!recvcounts || !displs || nrep < 0 || nranks <= 0 || nbin < 0 || item_width < 0)
+        return 1;
+    for (int r = 0; r < nranks; r++) {
+        int first, count;
+        dqmc_replica_rank_range(nrep, nranks, r, &first, &count);
+        const long long per = (long long)nbin * item_width;
+        const long long recv = per ? (long long)count * per : 0;
+        const long long disp = per ? (long long)first * per : 0;
+        if (recv > INT_MAX || disp > INT_MAX) return 1;
+        recvcounts[r] = (int)recv;
+        displs[r] = (int)disp;
+    }
+    return 0;
 }
 
 /* ------------------------------------------------------- bins, errors */

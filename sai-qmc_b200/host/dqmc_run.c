@@ -131,6 +131,17 @@ static int write_q(FILE *fp, const DqmcSpinPlan *plan, double breq, double beta,
 static const char *phase_names[] = {"bcache", "stack", "propose", "flush", "wrap", "bblock",
                                     "lmul", "combine", "green", "sdrift", "adopt", "measure"};
 
+/* Engine and local chain index of replica r of beta index b: engine k holds
+ * its replica range of every beta, beta-major. */
+static dqmc_engine *owner_of(dqmc_engine **engs, int neng, int nrep, int b, int r, int *local)
+{
+    const int k = dqmc_replica_rank_for_replica(nrep, neng, r);
+    int first, count;
+    dqmc_replica_rank_range(nrep, neng, k, &first, &count);
+    *local = b * count + (r - first);
+    return engs[k];
+}
+
 int dqmc_host_run(const char *input)
 {
     DqmcParams p;
@@ -179,7 +190,8 @@ int dqmc_host_run(const char *input)
     FILE *scalar = NULL, *replica_fp = NULL, *szz_fp = NULL, *sperp_fp = NULL, *cons_fp = NULL;
     FILE *prof_fp = NULL;
     DqmcSpinPlan zplan = {0}, pplan = {0};
-    dqmc_engine *eng = NULL;
+    dqmc_engine *engs[DQMC_MAX_GPUS] = {0};
+    int neng = 1, devs[DQMC_MAX_GPUS];
     double *scal = NULL, *zz = NULL, *pp = NULL, *series = NULL, *zbins = NULL, *pbins = NULL;
     unsigned long long *seeds = NULL;
     int *Ltrs = NULL;
@@ -373,10 +385,15 @@ int dqmc_host_run(const char *input)
     }
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
+    if (p.ngpu > 0) {
+        neng = p.ngpu;
+        for (int k = 0; k < neng; k++) devs[k] = p.gpu_devices[k];
+    } else {
+        devs[0] = p.gpu_device;
+    }
     if (nb_ok > 0) {
         dqmc_engine_desc d;
         dqmc_desc_default(&d);
-        d.device = p.gpu_device;
         d.precision = !strcmp(p.precision, "mixed") ? DQMC_PREC_MIXED : DQMC_PREC_FP64;
         d.delay_rank = p.delay_rank;
         d.sweep_order = !strcmp(p.sweep_order, "alternating") ? DQMC_SWEEP_ALTERNATING
@@ -385,40 +402,53 @@ int dqmc_host_run(const char *input)
                           : !strcmp(p.green_rebuild, "centered") ? DQMC_REBUILD_CENTERED
                                                                  : DQMC_REBUILD_COMBINE;
         d.drift = DQMC_DRIFT_STAB | (p.stab_drift_file[0] ? DQMC_DRIFT_SCRATCH : 0);
-        eng = dqmc_engine_create(&d);
-        if (!eng) {
-            fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
-            goto out;
-        }
-        const int model = dqmc_model_add(eng, L.n, L.has_coordinates ? L.Lx : 0,
-                                          L.has_coordinates ? L.Ly : 0, L.t, L.bipart, p.U, p.dtau);
-        if (model < 0 ||
-            dqmc_model_set_spin(eng, model, zplan.enabled ? zplan.nq : 0, zplan.mx, zplan.my,
-                                sp->enabled ? sp->nq : 0, sp->mx, sp->my)) {
-            fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
-            goto out;
-        }
-        for (int b = 0; b < nb_ok; b++)
-            for (int r = 0; r < nrep; r++)
-                if (dqmc_chain_add(eng, model, Ltrs[b], p.stab_interval, seeds[b * nrep + r],
-                                   NULL) < 0) {
-                    fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
-                    goto out;
-                }
-        const int per = p.nmeas / nbin;
-        if (dqmc_engine_prepare(eng, nbin) || dqmc_sweep(eng, p.nwarm)) {
-            fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
-            goto out;
-        }
-        for (int bi = 0; bi < nbin; bi++)
-            if (dqmc_sweep_measure(eng, per, bi)) {
+        /* one engine per device; device k owns replicas [first_k, first_k +
+         * count_k) of every beta (src/replica_mpi.c:13-37 with devices as
+         * ranks); all engines advance together (asynchronous launches) */
+        for (int k = 0; k < neng; k++) {
+            int first, count;
+            dqmc_replica_rank_range(nrep, neng, k, &first, &count);
+            if (count == 0) continue;
+            d.device = devs[k];
+            engs[k] = dqmc_engine_create(&d);
+            if (!engs[k]) {
                 fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
                 goto out;
             }
-        if (dqmc_synchronize(eng)) {
-            fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
-            goto out;
+            const int model =
+                dqmc_model_add(engs[k], L.n, L.has_coordinates ? L.Lx : 0,
+                               L.has_coordinates ? L.Ly : 0, L.t, L.bipart, p.U, p.dtau);
+            if (model < 0 ||
+                dqmc_model_set_spin(engs[k], model, zplan.enabled ? zplan.nq : 0, zplan.mx,
+                                    zplan.my, sp->enabled ? sp->nq : 0, sp->mx, sp->my)) {
+                fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                goto out;
+            }
+            for (int b = 0; b < nb_ok; b++)
+                for (int r = first; r < first + count; r++)
+                    if (dqmc_chain_add(engs[k], model, Ltrs[b], p.stab_interval,
+                                       seeds[b * nrep + r], NULL) < 0) {
+                        fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                        goto out;
+                    }
         }
+        const int per = p.nmeas / nbin;
+        for (int k = 0; k < neng; k++)
+            if (engs[k] && (dqmc_engine_prepare(engs[k], nbin) || dqmc_sweep(engs[k], p.nwarm))) {
+                fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                goto out;
+            }
+        for (int bi = 0; bi < nbin; bi++)
+            for (int k = 0; k < neng; k++)
+                if (engs[k] && dqmc_sweep_measure(engs[k], per, bi)) {
+                    fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                    goto out;
+                }
+        for (int k = 0; k < neng; k++)
+            if (engs[k] && dqmc_synchronize(engs[k])) {
+                fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                goto out;
+            }
     }
     clock_gettime(CLOCK_MONOTONIC, &t1);
     const double wall = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
@@ -435,8 +465,10 @@ int dqmc_host_run(const char *input)
         unsigned long long pcyc[12] = {0};
         for (int r = 0; r < nrep; r++) {
             const int c = b * nrep + r;
+            int lc;
+            dqmc_engine *e = owner_of(engs, neng, nrep, b, r, &lc);
             dqmc_chain_counters cnt;
-            dqmc_read_counters(eng, c, &cnt);
+            dqmc_read_counters(e, lc, &cnt);
             if (cnt.status) {
                 fprintf(stderr,
                         "ERROR: dqmc numerical breakdown (beta_index=%d beta=%.17g T=%.17g "
@@ -461,16 +493,25 @@ int dqmc_host_run(const char *input)
             }
             if (prof_fp) {
                 unsigned long long cy[12];
-                dqmc_read_profile(eng, c, cy, 12);
+                dqmc_read_profile(e, lc, cy, 12);
                 for (int k = 0; k < 12; k++) pcyc[k] += cy[k];
             }
         }
         if (replica_fp) {
             for (int r = 0; r < nrep; r++) {
+                int lc;
+                dqmc_engine *e = owner_of(engs, neng, nrep, b, r, &lc);
                 dqmc_chain_counters cnt;
-                dqmc_read_counters(eng, b * nrep + r, &cnt);
-                fprintf(replica_fp, "%.17g %.17g %d %llu %d %d %d %s\n", beta, T, r,
-                        seeds[b * nrep + r], p.nwarm, p.nmeas, nbin, cnt.status ? "error" : "ok");
+                dqmc_read_counters(e, lc, &cnt);
+                if (neng > 1) /* the owner column of the MPI runner (src/main.c:1216-1232) */
+                    fprintf(replica_fp, "%.17g %.17g %d %llu %d %d %d %s %d\n", beta, T, r,
+                            seeds[b * nrep + r], p.nwarm, p.nmeas, nbin,
+                            cnt.status ? "error" : "ok",
+                            dqmc_replica_rank_for_replica(nrep, neng, r));
+                else
+                    fprintf(replica_fp, "%.17g %.17g %d %llu %d %d %d %s\n", beta, T, r,
+                            seeds[b * nrep + r], p.nwarm, p.nmeas, nbin,
+                            cnt.status ? "error" : "ok");
             }
             fflush(replica_fp);
         }
@@ -478,8 +519,9 @@ int dqmc_host_run(const char *input)
         double *Eh = series, *Eg = Eh + total, *Ep = Eg + total, *Nn = Ep + total,
                *Dd = Nn + total, *Ss = Dd + total, *Ac = Ss + total;
         for (int r = 0; r < nrep; r++) {
-            const int c = b * nrep + r;
-            dqmc_read_bins(eng, c, scal, zz, pp);
+            int lc;
+            dqmc_engine *e = owner_of(engs, neng, nrep, b, r, &lc);
+            dqmc_read_bins(e, lc, scal, zz, pp);
             for (int bi = 0; bi < nbin; bi++) {
                 const int o = r * nbin + bi;
                 const double *bf = scal + (size_t)bi * DQMC_BIN_NFIELDS;
@@ -561,7 +603,8 @@ int dqmc_host_run(const char *input)
     }
     rc = 0;
 out:
-    if (eng) dqmc_engine_destroy(eng);
+    for (int k = 0; k < DQMC_MAX_GPUS; k++)
+        if (engs[k]) dqmc_engine_destroy(engs[k]);
     if (scalar) fclose(scalar);
     if (replica_fp) fclose(replica_fp);
     if (szz_fp) fclose(szz_fp);

@@ -134,3 +134,26 @@ def test_cli_alternating_matches_reference(tmp_path):
         a, b = table(gdir / name), table(rdir / name)
         assert a.shape == b.shape
         np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-9, err_msg=name)
+
+
+def test_cli_replicas_split_over_devices(tmp_path):
+    """gpu_devices: each listed device runs its contiguous replica range of
+    every beta (the reference's MPI split, src/replica_mpi.c:13-37); two
+    engines on the one device give the same outputs as one engine, and
+    replicas.dat gains the owner column of the MPI runner."""
+    one, two = tmp_path / "one", tmp_path / "two"
+    one.mkdir()
+    two.mkdir()
+    extra = "nrep=3\nreplica_log=replicas.dat\n"
+    run(EXE, one, extra)
+    run(EXE, two, extra + "gpu_devices=0,0\n")
+    for name in ("observables.dat", "szz.dat", "sperp.dat", "consistency.dat"):
+        a = [l for l in open(one / name) if not l.startswith("#")]
+        b = [l for l in open(two / name) if not l.startswith("#")]
+        assert a == b, name
+    ra = [l.split() for l in open(one / "replicas.dat") if not l.startswith("#")]
+    rb = [l.split() for l in open(two / "replicas.dat") if not l.startswith("#")]
+    assert len(ra) == len(rb) == 9
+    for x, y in zip(ra, rb):
+        assert len(x) == 8 and len(y) == 9 and x == y[:8]
+        assert int(y[8]) == (0 if int(y[2]) < 2 else 1)

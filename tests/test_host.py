@@ -28,7 +28,7 @@ class Params(C.Structure):
                 ("sperp_q", C.c_char * 256), ("sperp_file", C.c_char * 256),
                 ("spin_consistency_file", C.c_char * 256), ("seed", C.c_ulonglong),
                 ("delay_rank", C.c_int), ("precision", C.c_char * 16),
-                ("gpu_device", C.c_int)]
+                ("gpu_device", C.c_int), ("gpu_devices", C.c_int * 16), ("ngpu", C.c_int)]
 
 
 class Lattice(C.Structure):
@@ -79,7 +79,34 @@ def test_defaults_and_engine_keys(L, tmp_path):
     rc, p = read(L, tmp_path, "# only comments\n\nU = 7\n")   # 'U = 7' is not key=value
     assert rc == 0 and p.U == 4.0 and p.nbeta == 1 and p.beta_list[0] == 2.0
     rc, p = read(L, tmp_path, "delay_rank=16\nprecision=mixed\ngpu_device=0\n")
-    assert rc == 0 and p.delay_rank == 16 and p.precision == b"mixed"
+    assert rc == 0 and p.delay_rank == 16 and p.precision == b"mixed" and p.ngpu == 0
+    rc, p = read(L, tmp_path, "gpu_devices=0,3,1\n")
+    assert rc == 0 and p.ngpu == 3 and list(p.gpu_devices)[:3] == [0, 3, 1]
+    for bad in ("gpu_devices=0,-1\n", "gpu_devices=a\n", "gpu_devices=" + ",".join(["0"] * 17) + "\n"):
+        assert read(L, tmp_path, bad)[0] == 1
+
+
+def test_replica_ownership_matches_reference(L):
+    """The reference's own vectors for its MPI replica split
+    (tests/test_mpi_replica.c:27-66)."""
+    L.dqmc_replica_rank_range.argtypes = [C.c_int] * 3 + [C.POINTER(C.c_int)] * 2
+    L.dqmc_replica_gather_layout.argtypes = [C.c_int] * 4 + [C.c_void_p] * 2
+    first, count = C.c_int(), C.c_int()
+
+    def rr(nrep, nranks, rank):
+        L.dqmc_replica_rank_range(nrep, nranks, rank, C.byref(first), C.byref(count))
+        return first.value, count.value
+
+    assert [rr(10, 3, r) for r in range(3)] == [(0, 4), (4, 3), (7, 3)]
+    assert [rr(2, 4, r) for r in range(4)] == [(0, 1), (1, 1), (2, 0), (2, 0)]
+    owners = {(10, 3, 0): 0, (10, 3, 3): 0, (10, 3, 4): 1, (10, 3, 7): 2, (2, 4, 0): 0,
+              (2, 4, 1): 1, (10, 3, 10): -1, (0, 2, 0): -1}
+    for args, want in owners.items():
+        assert L.dqmc_replica_rank_for_replica(*args) == want
+    rc, dp = np.zeros(4, np.int32), np.zeros(4, np.int32)
+    assert L.dqmc_replica_gather_layout(5, 2, 3, 8, rc.ctypes.data, dp.ctypes.data) == 0
+    assert list(rc[:3]) == [32, 32, 16] and list(dp[:3]) == [0, 32, 64]
+    assert L.dqmc_replica_gather_layout(2 ** 31 - 1, 2, 1, 2, rc.ctypes.data, dp.ctypes.data) != 0
 
 
 @pytest.mark.parametrize("text", ["bogus=1\n", "nbin=1\n", "nmeas=10\nnbin=3\n", "U=-1\n",
