@@ -46,6 +46,27 @@ enum { DQMC_DRIFT_STAB = 1, DQMC_DRIFT_SCRATCH = 2 };
  * The proposals and their order are the same in all three. */
 enum { DQMC_PAIRS_AUTO = 0, DQMC_PAIRS_OFF = 1, DQMC_PAIRS_ON = 2 };
 
+/* UDV scale records (src/dqmc.c:100-378): where a factor was observed, as
+ * the reference's direction strings, and the record layout returned by
+ * dqmc_read_udv_records.  Per factor: min and max of log|D| over the finite
+ * nonzero entries, and the counts of finite nonzero, zero and non-finite
+ * entries (udv_scale_stats, src/dqmc.c:108-142). */
+enum {
+    DQMC_UDV_STACK_SUFFIX_PRE_RMUL = 0,  /* "stack_suffix_pre_rmul" (green.c:214) */
+    DQMC_UDV_STACK_PREFIX_PRE_LMUL = 1,  /* "stack_prefix_pre_lmul" (green.c:238) */
+    DQMC_UDV_FORWARD = 2,                /* "forward" boundary pair (dqmc.c:707)    */
+    DQMC_UDV_BACKWARD = 3,               /* "backward" boundary pair (dqmc.c:831)   */
+    DQMC_UDV_LEFT_FORWARD = 4,           /* "left_udv_forward" (dqmc.c:772)         */
+    DQMC_UDV_LEFT_BACKWARD = 5           /* "left_udv_backward" (dqmc.c:926)        */
+};
+enum {
+    DQMC_UDV_R_KIND = 0, DQMC_UDV_R_TAU, DQMC_UDV_R_BOUNDARY, DQMC_UDV_R_SWEEP,
+    DQMC_UDV_R_LEFT = 4,    /* min, max, finite, zero, nonfinite of the (left) factor */
+    DQMC_UDV_R_RIGHT = 9,   /* the same for the right factor of a boundary pair      */
+    DQMC_UDV_R_HAS_RIGHT = 14,
+    DQMC_UDV_RECORD_DOUBLES = 16
+};
+
 /* Per-bin scalar layout returned by dqmc_read_bins (src/replica.h:6-16). */
 enum {
     DQMC_BIN_SUM_SIGN_EHUB = 0,
@@ -74,7 +95,11 @@ typedef struct {
     int green_rebuild; /* DQMC_REBUILD_*                                    */
     int flush_pairs; /* DQMC_PAIRS_*: stage two consecutive site blocks and
                         update G once for both (rank <= 2k)               */
-    int reserved[4];
+    int udv_diag;    /* 1: record the UDV scale statistics of every factor
+                        the reference's udv_scale_file / udv_centered_file
+                        diagnostics report (dqmc_read_udv_records); the
+                        sweeps then run one launch per sweep             */
+    int reserved[3];
 } dqmc_engine_desc;
 
 typedef struct {
@@ -232,6 +257,12 @@ int dqmc_expm_sym(int n, const double *A, double scale, double *out);
 #define DQMC_NOALLOC_MAX_N 128
 int dqmc_udv_green_noalloc(int device, int n, const double *U, const double *D,
                            const double *T, double *G, int *det_sign);
+
+/* Moves up to max_records of a chain's UDV scale records (in the order
+ * they were taken, DQMC_UDV_RECORD_DOUBLES each) to out and returns how
+ * many, or -1 on error; records beyond max_records stay for the next call.
+ * Needs dqmc_engine_desc.udv_diag. */
+int dqmc_read_udv_records(dqmc_engine *e, int chain, double *out, int max_records);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,10 @@ typedef struct {
     int alt, dir, pvalid, svalid;
     int rebuild;               /* 0: combine, 1: two-sided G at boundaries */
     int pair;                  /* flush G after every second site block   */
+    /* UDV scale records (opt-in): DQMC_UDV_RECORD_DOUBLES each, udv_n of
+     * udv_cap used since the host last drained them, udv_lost dropped */
+    int udv_cap, udv_n, udv_lost;
+    double *udvrec;
     double sign;
     unsigned long long attempts, accepted, sweeps;
     unsigned long long meas_accepted, meas_attempts;  /* counters at last measurement */

@@ -9,6 +9,7 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdarg>
@@ -124,7 +125,13 @@ struct HChain {
     int model, L, stab, M, kb;
     uint64_t rng[4];
     std::vector<signed char> field;
+    std::vector<double> udv;   /* drained UDV scale records, oldest first */
 };
+
+/* UDV scale records a chain can take in one sweep: M - 1 stack factors,
+ * M - 1 boundaries, the final factor, and M prefix factors of a backward
+ * sweep that has to build its prefix stack. */
+int udv_cap(int M) { return 3 * M + 4; }
 
 }  // namespace
 
@@ -503,6 +510,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += rup((size_t)c.M * nn * 8);                     /* bcache */
         off += 6 * rup(nn * 8);                               /* w */
         off += 2 * rup((size_t)n * 2 * c.kb * 8);             /* Zs, Ys */
+        if (e->desc.udv_diag)                                  /* UDV scale records */
+            off += rup((size_t)udv_cap(c.M) * DQMC_UDV_RECORD_DOUBLES * 8);
         off += rup((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB * DQMC_QNB * 8);
         off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
@@ -554,6 +563,10 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         for (int i = 0; i < 6; ++i) d.w[i] = (double *)take(nn * 8);
         d.Zs = (double *)take((size_t)n * 2 * c.kb * 8);
         d.Ys = (double *)take((size_t)n * 2 * c.kb * 8);
+        if (e->desc.udv_diag) {
+            d.udv_cap = udv_cap(c.M);
+            d.udvrec = (double *)take((size_t)d.udv_cap * DQMC_UDV_RECORD_DOUBLES * 8);
+        }
         d.twall = (double *)take((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB *
                                  DQMC_QNB * 8);
         d.bins = (double *)take((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
@@ -604,19 +617,70 @@ static int kflags(const dqmc_engine *e)
            (e->desc.precision == DQMC_PREC_MIXED ? dq::KF_MIXED : 0);
 }
 
+static int chain_ok(dqmc_engine *e, int chain, const char *who);
+
+/* Moves every chain's device UDV scale records to its host list (after
+ * each sweep launch when the records are on: a launch of one sweep fills
+ * at most udv_cap records per chain). */
+static int udv_drain(dqmc_engine *e)
+{
+    if (!e->desc.udv_diag) return 0;
+    CU(cudaStreamSynchronize(e->stream));
+    for (size_t c = 0; c < e->chains.size(); ++c) {
+        int cnt[3];   /* udv_cap, udv_n, udv_lost */
+        CU(cudaMemcpy(cnt, (char *)(e->dchains + c) + offsetof(DqmcChainDev, udv_cap),
+                      sizeof cnt, cudaMemcpyDeviceToHost));
+        if (cnt[2]) return set_err("UDV scale records lost (chain %zu)", c);
+        if (cnt[1] <= 0) continue;
+        std::vector<double> &h = e->chains[c].udv;
+        const size_t old = h.size(), add = (size_t)cnt[1] * DQMC_UDV_RECORD_DOUBLES;
+        h.resize(old + add);
+        CU(cudaMemcpy(h.data() + old, e->hdev[c].udvrec, add * 8, cudaMemcpyDeviceToHost));
+        const int zero = 0;
+        CU(cudaMemcpy((char *)(e->dchains + c) + offsetof(DqmcChainDev, udv_n), &zero,
+                      sizeof zero, cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
 int dqmc_sweep(dqmc_engine *e, int nsweeps)
 {
     if (check_prepared(e, "dqmc_sweep")) return 1;
     if (nsweeps <= 0) return 0;
     const unsigned nc = (unsigned)e->chains.size();
-    ev_begin(e, 0);
-    if (e->per_sm == 2)
-        dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), nsweeps);
-    else
-        dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, kflags(e), nsweeps);
-    ev_end(e);
-    CU(cudaGetLastError());
+    /* with UDV scale records, one launch per sweep, drained in between */
+    const int per = e->desc.udv_diag ? 1 : nsweeps;
+    for (int done = 0; done < nsweeps; done += per) {
+        ev_begin(e, 0);
+        if (e->per_sm == 2)
+            dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), per);
+        else
+            dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, kflags(e), per);
+        ev_end(e);
+        CU(cudaGetLastError());
+        if (udv_drain(e)) return 1;
+    }
     return 0;
+}
+
+int dqmc_read_udv_records(dqmc_engine *e, int chain, double *out, int max_records)
+{
+    if (chain_ok(e, chain, "dqmc_read_udv_records")) return -1;
+    if (!e->desc.udv_diag) {
+        set_err("dqmc_read_udv_records: engine created without udv_diag");
+        return -1;
+    }
+    if (max_records < 0 || (max_records > 0 && !out)) {
+        set_err("dqmc_read_udv_records: bad output buffer");
+        return -1;
+    }
+    std::vector<double> &h = e->chains[chain].udv;
+    const int have = (int)(h.size() / DQMC_UDV_RECORD_DOUBLES);
+    const int k = have < max_records ? have : max_records;
+    const size_t nd = (size_t)k * DQMC_UDV_RECORD_DOUBLES;
+    std::copy(h.begin(), h.begin() + nd, out);
+    h.erase(h.begin(), h.begin() + nd);
+    return k;
 }
 
 int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
@@ -632,6 +696,7 @@ int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
         else
             dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, f, 1);
         ev_end(e);
+        if (udv_drain(e)) return 1;
         ev_begin(e, 1);
         dq::launch_measure(nc, e->msmem, e->stream, e->dchains, e->dmodels, bin);
         ev_end(e);

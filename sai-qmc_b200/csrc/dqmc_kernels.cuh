@@ -1,6 +1,7 @@
 /* Sweep, measurement and test kernels.  One CTA = one chain. */
 #pragma once
 #include "dqmc_device.cuh"
+#include "dqmc_gpu.h"
 #include "dqmc_mixed.cuh"
 
 namespace DQMC_NS {
@@ -439,6 +440,92 @@ __device__ __noinline__ int green_scratch(DqmcChainDev *ch, const DqmcModelDev &
     return *flag ? 0 : ds;
 }
 
+/* Statistics of log|D| of one UDV factor (udv_scale_stats, dqmc.c:108-142,
+ * on the log-scale D held here: ell = -inf is a zero entry, +inf or NaN a
+ * non-finite one): o = {min, max over finite entries (NaN if none),
+ * finite, zero, non-finite counts}, valid in thread 0.  All threads call. */
+__device__ void ell_stats(int n, const double *ell, double *o, Smem &s)
+{
+    static_assert(5 * NW <= 40, "reduction slots");
+    double mn = INFINITY, mx = -INFINITY, fin = 0.0, zero = 0.0, bad = 0.0;
+    for (int e = threadIdx.x; e < n; e += NT) {
+        const double x = ell[e];
+        if (x == -INFINITY) {
+            zero += 1.0;
+        } else if (isfinite(x)) {
+            fin += 1.0;
+            mn = fmin(mn, x);
+            mx = fmax(mx, x);
+        } else {
+            bad += 1.0;
+        }
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(FULL, mn, d));
+        mx = fmax(mx, __shfl_xor_sync(FULL, mx, d));
+        fin += __shfl_xor_sync(FULL, fin, d);
+        zero += __shfl_xor_sync(FULL, zero, d);
+        bad += __shfl_xor_sync(FULL, bad, d);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        double *r = s.red + 5 * warp;
+        r[0] = mn;
+        r[1] = mx;
+        r[2] = fin;
+        r[3] = zero;
+        r[4] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < NW; ++w) {
+            const double *r = s.red + 5 * w;
+            mn = fmin(mn, r[0]);
+            mx = fmax(mx, r[1]);
+            fin += r[2];
+            zero += r[3];
+            bad += r[4];
+        }
+        o[0] = fin > 0.0 ? mn : NAN;
+        o[1] = fin > 0.0 ? mx : NAN;
+        o[2] = fin;
+        o[3] = zero;
+        o[4] = bad;
+    }
+    __syncthreads();
+}
+
+/* One UDV scale record (dqmc_record_udv_scale_diag / _single_, dqmc.c:
+ * 196-230) of the factor L (and R for a boundary pair) into the chain's
+ * record buffer; a no-op unless the engine enabled the records. */
+__device__ __noinline__ void udv_record(DqmcChainDev *ch, int kind, int tau, int boundary, int n,
+                                        const double *ellL, const double *ellR, Smem &s)
+{
+    if (!ch->udvrec) return;
+    double a[5], b[5] = {NAN, NAN, 0.0, 0.0, 0.0};
+    ell_stats(n, ellL, a, s);
+    if (ellR) ell_stats(n, ellR, b, s);
+    if (threadIdx.x == 0) {
+        if (ch->udv_n < ch->udv_cap) {
+            double *r = ch->udvrec + (size_t)ch->udv_n * DQMC_UDV_RECORD_DOUBLES;
+            r[DQMC_UDV_R_KIND] = kind;
+            r[DQMC_UDV_R_TAU] = tau;
+            r[DQMC_UDV_R_BOUNDARY] = boundary;
+            r[DQMC_UDV_R_SWEEP] = (double)ch->sweeps;
+            for (int k = 0; k < 5; ++k) {
+                r[DQMC_UDV_R_LEFT + k] = a[k];
+                r[DQMC_UDV_R_RIGHT + k] = b[k];
+            }
+            r[DQMC_UDV_R_HAS_RIGHT] = ellR ? 1.0 : 0.0;
+            r[DQMC_UDV_R_HAS_RIGHT + 1] = 0.0;
+            ch->udv_n++;
+        } else {
+            ch->udv_lost++;
+        }
+    }
+}
+
 /* The forward sweep, dqmc_sweep_forward (dqmc.c:609-813) with
  * carry_prefix = 0, use_ph = 1 and the combine rebuild.  Returns false on a
  * numerical failure (flag holds the reason). */
@@ -475,6 +562,8 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         udv_identity(Sj(M), n);
         for (int j = M - 1; j >= 1; --j) {
             udv_copy(Sj(j), Sj(j + 1), n);
+            udv_record(ch, DQMC_UDV_STACK_SUFFIX_PRE_RMUL, min(j * stab, L), j, n, Sj(j).ell,
+                       nullptr, s);
             udv_rmul(n, Sj(j), ch->bcache + j * nn, w, s, flag);
             if (*flag) return false;
         }
@@ -528,6 +617,11 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         }
         tau_left = te;
         if (alt) udv_copy(Pj(boundary ? (l + 1) / stab : M), left, n);   /* dqmc.c:704-706,767 */
+        if (boundary)   /* dqmc.c:707-715, 772-779 */
+            udv_record(ch, DQMC_UDV_FORWARD, l + 1, (l + 1) / stab, n, left.ell,
+                       Sj((l + 1) / stab).ell, s);
+        else
+            udv_record(ch, DQMC_UDV_LEFT_FORWARD, L, M, n, left.ell, nullptr, s);
         int ds;
         if (boundary && ch->rebuild) {
             ds = udv_green2(n, left, Sj((l + 1) / stab), Gn, tmp2, w, s, flag);
@@ -589,6 +683,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
             bblock(n, b0, b1 - b0, ch->field, md.expK, v0, v1, ch->bcache + (j - 1) * nn, tmp,
                    tmp2, s);
             udv_copy(Pj(j), Pj(j - 1), n);
+            udv_record(ch, DQMC_UDV_STACK_PREFIX_PRE_LMUL, b1, j, n, Pj(j).ell, nullptr, s);
             udv_lmul(n, Pj(j), ch->bcache + (j - 1) * nn, nullptr, nullptr, 0.0, 0.0, w, s,
                      flag);
             if (*flag) return false;
@@ -627,6 +722,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
         int ds;
         if (boundary) {
             udv_copy(Sj(j), u, n);
+            udv_record(ch, DQMC_UDV_BACKWARD, tau, j, n, Pj(j).ell, u.ell, s);   /* dqmc.c:831 */
             if (ch->rebuild) {
                 ds = udv_green2(n, Pj(j), u, Gn, tmp2, w, s, flag);
             } else {
@@ -636,6 +732,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
                 ds = udv_green(n, comb, Gn, w, s, flag);
             }
         } else {
+            udv_record(ch, DQMC_UDV_LEFT_BACKWARD, 0, 0, n, u.ell, nullptr, s);   /* dqmc.c:926 */
             ds = udv_green(n, u, Gn, w, s, flag);
         }
         pc.charge(ch, DQMC_PH_GREEN);

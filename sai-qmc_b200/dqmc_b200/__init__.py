@@ -23,6 +23,9 @@ SWEEP_FORWARD, SWEEP_ALTERNATING = 0, 1
 REBUILD_COMBINE, REBUILD_TWO_SIDED, REBUILD_CENTERED = 0, 1, 2
 DRIFT_STAB, DRIFT_SCRATCH = 1, 2
 PAIRS_AUTO, PAIRS_OFF, PAIRS_ON = 0, 1, 2
+UDV_DIRECTIONS = ["stack_suffix_pre_rmul", "stack_prefix_pre_lmul", "forward", "backward",
+                  "left_udv_forward", "left_udv_backward"]
+UDV_RECORD_DOUBLES = 16
 BIN_FIELDS = ["sum_sign_Ehub", "sum_sign_Egc", "sum_sign_Eph", "sum_sign_N",
               "sum_sign_D", "sum_sign", "count", "accepted", "attempts"]
 NBIN_FIELDS = len(BIN_FIELDS)
@@ -38,7 +41,7 @@ class Desc(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int),
                 ("delay_rank", C.c_int), ("drift", C.c_int),
                 ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("green_rebuild", C.c_int),
-                ("flush_pairs", C.c_int), ("reserved", C.c_int * 4)]
+                ("flush_pairs", C.c_int), ("udv_diag", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class Counters(C.Structure):
@@ -106,6 +109,7 @@ def lib():
     L.dqmc_write_green.argtypes = [C.c_void_p, C.c_int, _dp]
     L.dqmc_write_rng.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_uint64)]
     L.dqmc_expm_sym.argtypes = [C.c_int, _dp, C.c_double, _dp]
+    L.dqmc_read_udv_records.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
     L.dqmc_udv_green_noalloc.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                          C.POINTER(C.c_int)]
     _lib = L
@@ -198,7 +202,7 @@ class Engine:
 
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
                  drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD,
-                 green_rebuild=REBUILD_COMBINE, flush_pairs=PAIRS_AUTO):
+                 green_rebuild=REBUILD_COMBINE, flush_pairs=PAIRS_AUTO, udv_diag=0):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
@@ -207,6 +211,7 @@ class Engine:
         d.sweep_order = sweep_order
         d.green_rebuild = green_rebuild
         d.flush_pairs = flush_pairs
+        d.udv_diag = udv_diag
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
             raise DqmcError(L.dqmc_last_error().decode())
@@ -299,6 +304,20 @@ class Engine:
         return (sc.reshape(self.nbin, NBIN_FIELDS),
                 zz[: self.nbin * m["nq_zz"]].reshape(self.nbin, m["nq_zz"]),
                 pp[: self.nbin * m["nq_perp"]].reshape(self.nbin, m["nq_perp"]))
+
+    def udv_records(self, c):
+        """The chain's UDV scale records since the last call (needs
+        udv_diag=1): rows of UDV_RECORD_DOUBLES, see include/dqmc_gpu.h."""
+        out = []
+        buf = np.zeros(256 * UDV_RECORD_DOUBLES)
+        while True:
+            k = lib().dqmc_read_udv_records(self.h, c, buf.ctypes.data, 256)
+            if k < 0:
+                raise DqmcError(lib().dqmc_last_error().decode())
+            if k == 0:
+                break
+            out.append(buf[: k * UDV_RECORD_DOUBLES].reshape(k, UDV_RECORD_DOUBLES).copy())
+        return np.concatenate(out) if out else np.zeros((0, UDV_RECORD_DOUBLES))
 
     def profile(self, c):
         """Per-phase SM cycles of chain c (PHASES order)."""

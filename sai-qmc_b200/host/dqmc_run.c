@@ -6,6 +6,7 @@
  * instead of one CPU process/thread per replica and beta after beta.
  */
 #define _XOPEN_SOURCE 700
+#include <float.h>
 #include <limits.h>
 #include <math.h>
 #include <stdarg.h>
@@ -131,6 +132,125 @@ static int write_q(FILE *fp, const DqmcSpinPlan *plan, double breq, double beta,
 static const char *phase_names[] = {"bcache", "stack", "propose", "flush", "wrap", "bblock",
                                     "lmul", "combine", "green", "sdrift", "adopt", "measure"};
 
+static int udv_header(const char *path, const char *what, const char *header)
+{
+    FILE *f = fopen(path, "w");
+    if (!f) {
+        fprintf(stderr, "ERROR: failed to open %s %s\n", what, path);
+        return 1;
+    }
+    fputs(header, f);
+    if (fclose(f)) {
+        fprintf(stderr, "ERROR: failed to close %s %s\n", what, path);
+        return 1;
+    }
+    return 0;
+}
+
+static const char *udv_direction(int kind)
+{
+    static const char *names[] = {"stack_suffix_pre_rmul", "stack_prefix_pre_lmul", "forward",
+                                  "backward", "left_udv_forward", "left_udv_backward"};
+    return kind >= 0 && kind < 6 ? names[kind] : "?";
+}
+
+/* One replica's UDV scale records as the reference's diagnostic lines:
+ * udv_scale_file rows of dqmc_write_udv_scale_diag (src/dqmc.c:158-194) and
+ * udv_centered_file rows of dqmc_record_udv_centered_diag (src/dqmc.c:
+ * 287-340).  The engine holds log|D| itself, so effective log D, radius and
+ * margin are its own; the stored/offset split of the reference's centered
+ * representation is taken as recentered at the record (offset = midpoint of
+ * the log D range).  A centered factor that is invalid (zero or non-finite
+ * D) or within 8 of the log(DBL_MAX) margin fails the run, as the
+ * reference's diagnostic failure stops the replica. */
+static int write_udv_records(const DqmcParams *p, dqmc_engine *e, int chain, int b, int Ltr,
+                             int r, unsigned long long seed, int n)
+{
+    FILE *fs = p->udv_scale_file[0] ? fopen(p->udv_scale_file, "a") : NULL;
+    FILE *fc = p->udv_centered_file[0] ? fopen(p->udv_centered_file, "a") : NULL;
+    int rc = 0;
+    if ((p->udv_scale_file[0] && !fs) || (p->udv_centered_file[0] && !fc)) {
+        fprintf(stderr, "ERROR: failed to open %s %s\n",
+                fs ? "udv_centered_file" : "udv_scale_file",
+                fs ? p->udv_centered_file : p->udv_scale_file);
+        rc = 1;
+    }
+    double rec[64 * DQMC_UDV_RECORD_DOUBLES];
+    int k;
+    while (!rc && (k = dqmc_read_udv_records(e, chain, rec, 64)) > 0) {
+        for (int i = 0; i < k; i++) {
+            const double *x = rec + (size_t)i * DQMC_UDV_RECORD_DOUBLES;
+            const int kind = (int)x[DQMC_UDV_R_KIND], tau = (int)x[DQMC_UDV_R_TAU];
+            const int bnd = (int)x[DQMC_UDV_R_BOUNDARY];
+            const unsigned long long sw = (unsigned long long)x[DQMC_UDV_R_SWEEP];
+            const double *lf = x + DQMC_UDV_R_LEFT, *rt = x + DQMC_UDV_R_RIGHT;
+            const int pair = x[DQMC_UDV_R_HAS_RIGHT] != 0.0;
+            if (fs) {
+                const double lsp = lf[2] > 0 ? lf[1] - lf[0] : NAN;
+                const double rsp = rt[2] > 0 ? rt[1] - rt[0] : NAN;
+                const double cross =
+                    pair && isfinite(lf[1]) && isfinite(rt[1]) ? lf[1] + rt[1] : NAN;
+                fprintf(fs,
+                        "%d %d %d %llu %.17g %.17g %d %llu %d %d %s %s %.17g %.17g %.17g %d %d "
+                        "%d %.17g %.17g %.17g %d %d %d %.17g\n",
+                        b, Ltr, r, seed, p->U, p->dtau, p->stab_interval, sw, tau, bnd, "u",
+                        udv_direction(kind), lf[0], lf[1], lsp, (int)lf[2], (int)lf[3],
+                        (int)lf[4], rt[0], rt[1], rsp, (int)rt[2], (int)rt[3], (int)rt[4],
+                        cross);
+            }
+            if (fc) {
+                /* the centered factor: left_u, i.e. the right one of a
+                 * backward pair (src/dqmc.c:707-709, 831-833) */
+                const double *c = kind == DQMC_UDV_BACKWARD ? rt : lf;
+                const int valid = (int)c[2] == n && c[3] == 0 && c[4] == 0;
+                double smin = NAN, smax = NAN, rad = NAN, off = NAN, emin = NAN, emax = NAN,
+                       margin = NAN;
+                if (valid) {
+                    emin = c[0];
+                    emax = c[1];
+                    rad = 0.5 * (emax - emin);
+                    off = emin + rad;
+                    smin = emin - off;
+                    smax = emax - off;
+                    margin = log(DBL_MAX) - rad;
+                }
+                int warning = valid && margin <= 32.0;
+                const char *status = "ok";
+                int fail = 0;
+                if (!valid) {
+                    status = "invalid_factor";
+                    fail = 1;
+                } else if (margin <= 8.0) {
+                    status = "hard_fail_centered_radius";
+                    warning = 1;
+                    fail = 1;
+                } else if (warning) {
+                    status = "warning";
+                }
+                fprintf(fc,
+                        "%d %d %d %llu %llu %d %d %s %s %.17g %.17g %.17g %.17g %.17g %.17g "
+                        "%.17g %d %s\n",
+                        b, Ltr, r, seed, sw, tau, bnd, "u", udv_direction(kind), smin, smax, rad,
+                        off, emin, emax, margin, warning, status);
+                if (fail) {
+                    fprintf(stderr, "ERROR: centered UDV diagnostic failed (beta_index=%d "
+                                    "replica=%d sweep_count=%llu tau=%d status=%s)\n",
+                            b, r, sw, tau, status);
+                    rc = 1;
+                    break;
+                }
+            }
+        }
+    }
+    if (!rc && k < 0) {
+        fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+        rc = 1;
+    }
+    if (fs && fclose(fs)) rc = 1;
+    if (fc && fclose(fc)) rc = 1;
+    return rc;
+}
+
 /* Engine and local chain index of replica r of beta index b: engine k holds
  * its replica range of every beta, beta-major. */
 static dqmc_engine *owner_of(dqmc_engine **engs, int neng, int nrep, int b, int r, int *local)
@@ -213,15 +333,34 @@ int dqmc_host_run(const char *input)
         fprintf(stderr, "ERROR: stab_drift_file currently supports parallel=serial only\n");
         goto out;
     }
+    /* src/main.c:733-762 */
+    if (p.udv_scale_file[0] && strcmp(p.parallel, "serial")) {
+        fprintf(stderr, "ERROR: udv_scale_file currently supports parallel=serial only\n");
+        goto out;
+    }
+    if (p.udv_centered_file[0] && strcmp(p.parallel, "serial")) {
+        fprintf(stderr, "ERROR: udv_centered_file currently supports parallel=serial only\n");
+        goto out;
+    }
     if (p.udv_centered_file[0] && strcmp(p.green_rebuild, "centered")) {
         fprintf(stderr, "ERROR: udv_centered_file requires green_rebuild=centered\n");
         goto out;
     }
-    if (p.udv_scale_file[0] || p.udv_centered_file[0]) {
-        fprintf(stderr, "ERROR: the GPU engine does not write udv_scale_file / "
-                        "udv_centered_file diagnostics\n");
+    /* init_udv_scale_file / init_udv_centered_file (src/main.c:474-515) */
+    if (p.udv_scale_file[0] &&
+        udv_header(p.udv_scale_file, "udv_scale_file",
+                   "# beta_index Ltr replica_id seed U dtau stab_interval sweep_count tau "
+                   "boundary spin direction left_min_logD left_max_logD left_spread_logD "
+                   "left_finite_count left_zero_count left_nonfinite_count right_min_logD "
+                   "right_max_logD right_spread_logD right_finite_count right_zero_count "
+                   "right_nonfinite_count cross_max_logD\n"))
         goto out;
-    }
+    if (p.udv_centered_file[0] &&
+        udv_header(p.udv_centered_file, "udv_centered_file",
+                   "# beta_index Ltr replica_id seed sweep_count tau boundary spin direction "
+                   "stored_min_logD stored_max_logD stored_radius log_offset "
+                   "effective_min_logD effective_max_logD remaining_margin warning status\n"))
+        goto out;
     if (p.stab_drift_file[0]) {
         FILE *f = fopen(p.stab_drift_file, "w");
         if (!f) {
@@ -402,6 +541,7 @@ int dqmc_host_run(const char *input)
                           : !strcmp(p.green_rebuild, "centered") ? DQMC_REBUILD_CENTERED
                                                                  : DQMC_REBUILD_COMBINE;
         d.drift = DQMC_DRIFT_STAB | (p.stab_drift_file[0] ? DQMC_DRIFT_SCRATCH : 0);
+        d.udv_diag = p.udv_scale_file[0] || p.udv_centered_file[0];
         /* one engine per device; device k owns replicas [first_k, first_k +
          * count_k) of every beta (src/replica_mpi.c:13-37 with devices as
          * ranks); all engines advance together (asynchronous launches) */
@@ -491,6 +631,9 @@ int dqmc_host_run(const char *input)
                         cnt.scratch_drift_max_tau, cnt.scratch_drift_max_sweep, cnt.status ? 1 : 0);
                 fclose(f);
             }
+            if ((p.udv_scale_file[0] || p.udv_centered_file[0]) &&
+                write_udv_records(&p, e, lc, b, Ltrs[b], r, seeds[c], L.n))
+                goto out;
             if (prof_fp) {
                 unsigned long long cy[12];
                 dqmc_read_profile(e, lc, cy, 12);

@@ -184,3 +184,22 @@ def test_lattice_and_plans(L, tmp_path):
     lib.dqmc_spin_plan_free(C.byref(plan))
     lib.dqmc_lattice_free(C.byref(lat))
     lib.dqmc_lattice_free(C.byref(lat2))
+
+
+@pytest.mark.parametrize("extra,msg", [
+    ("udv_scale_file=s.dat\nparallel=omp\n", "udv_scale_file currently supports parallel=serial only"),
+    ("udv_centered_file=c.dat\nparallel=omp\n",
+     "udv_centered_file currently supports parallel=serial only"),
+    ("udv_centered_file=c.dat\n", "udv_centered_file requires green_rebuild=centered"),
+])
+def test_driver_rejects_diagnostics_like_reference(tmp_path, extra, msg):
+    """The reference's checks on the UDV diagnostic files (src/main.c:733-762),
+    made before any device work."""
+    import subprocess
+    exe = os.path.join(ROOT, "sai-qmc_b200", "dqmc_gpu")
+    if not os.path.exists(exe):
+        pytest.skip("dqmc_gpu not built")
+    (tmp_path / "input.txt").write_text("lattice=chain\nLx=4\npbc=1\n" + extra)
+    r = subprocess.run([exe, "input.txt"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 1 and msg in r.stderr
