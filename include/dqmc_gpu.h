@@ -211,6 +211,15 @@ int dqmc_read_bins(dqmc_engine *e, int chain, double *scalars, double *szz,
  * Copies min(count, 12) values. */
 int dqmc_read_profile(dqmc_engine *e, int chain, unsigned long long *cycles,
                       int count);
+/* Calls counted with the same phases: stack builds (bcache), suffix-stack
+ * rmuls (stack), accepted flips (propose), G updates (flush), wraps,
+ * B-block products, boundary UDV updates, combines, G from UDV, rebuilds
+ * from scratch, adoptions, measurements.  Copies min(count, 12) values. */
+int dqmc_read_profile_calls(dqmc_engine *e, int chain, unsigned long long *calls,
+                            int count);
+/* SM clock of the engine's device in Hz (its maximum), to turn the cycle
+ * counters into seconds; 0 on error. */
+double dqmc_clock_hz(dqmc_engine *e);
 /* Clears all bins of all chains. */
 int dqmc_clear_bins(dqmc_engine *e);
 

@@ -114,6 +114,11 @@ typedef struct {
     signed char *mix;
     int *mix_ex;
     unsigned long long prof[DQMC_PH_COUNT];
+    /* calls of each phase's region as the reference's profiler counts them
+     * (src/profiler.c): wraps, accepted flips and G updates, stack builds,
+     * B-block products, UDV updates, combines, G from UDV, adoptions,
+     * rebuilds from scratch, measurements */
+    unsigned long long pcalls[DQMC_PH_COUNT];
 } DqmcChainDev;
 
 /* UDV slot: U (n*n) | T (n*n) | ell = log D (n) | detU (1) | pad (1)        */

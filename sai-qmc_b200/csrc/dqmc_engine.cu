@@ -889,6 +889,24 @@ int dqmc_read_profile(dqmc_engine *e, int chain, unsigned long long *cycles, int
     return 0;
 }
 
+int dqmc_read_profile_calls(dqmc_engine *e, int chain, unsigned long long *calls, int count)
+{
+    if (chain_ok(e, chain, "dqmc_read_profile_calls")) return 1;
+    DqmcChainDev d;
+    CU(cudaStreamSynchronize(e->stream));
+    CU(cudaMemcpy(&d, e->dchains + chain, sizeof d, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < count && i < DQMC_PH_COUNT; ++i) calls[i] = d.pcalls[i];
+    return 0;
+}
+
+double dqmc_clock_hz(dqmc_engine *e)
+{
+    int khz = 0;
+    if (!e || cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, e->desc.device) != cudaSuccess)
+        return 0.0;
+    return 1e3 * khz;
+}
+
 int dqmc_clear_bins(dqmc_engine *e)
 {
     if (check_prepared(e, "dqmc_clear_bins")) return 1;

@@ -13,11 +13,12 @@ enum { KF_MEASURE = 1, KF_SDRIFT = 2, KF_STAB_DRIFT = 4, KF_MIXED = 8 };
 struct PhaseClock {
     long long t;
     __device__ __forceinline__ void mark() { t = clock64(); }
-    __device__ __forceinline__ void charge(DqmcChainDev *ch, int ph)
+    __device__ __forceinline__ void charge(DqmcChainDev *ch, int ph, unsigned calls = 0)
     {
         if (threadIdx.x == 0) {
             const long long now = clock64();
             ch->prof[ph] += (unsigned long long)(now - t);
+            ch->pcalls[ph] += calls;
             t = now;
         }
     }
@@ -159,6 +160,7 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
             for (int q = 0; q < 4; ++q) rng[q] = r4[q];
             *att += (unsigned long long)kbs;
             *acc += nacc;
+            ch->pcalls[DQMC_PH_PROPOSE] += nacc;   /* green_delay_accept calls */
             s.iscr[2 * DQMC_MAX_KB] = m;
         }
     }
@@ -170,7 +172,7 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
         gemm_nn_rmw(
             n, n, mA, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
             [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
-        pc.charge(ch, DQMC_PH_FLUSH);
+        pc.charge(ch, DQMC_PH_FLUSH, 1);
         return 0;
     }
     /* Tu = (I - F Su)^-1 (warp 0), Tv = (I + Sc)^-1 (warp 1); lane q owns
@@ -381,7 +383,7 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
     gemm_nn_rmw(
         n, n, mt, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
         [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
-    pc.charge(ch, DQMC_PH_FLUSH);
+    pc.charge(ch, DQMC_PH_FLUSH, 1);
     return 0;
 }
 
@@ -557,13 +559,14 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
                        tmp2, s);
             }
         }
-        pc.charge(ch, DQMC_PH_BCACHE);
+        pc.charge(ch, DQMC_PH_BCACHE, 1);
         /* suffix stack (green_stack_build_suffix, green.c:203-226) */
         udv_identity(Sj(M), n);
         for (int j = M - 1; j >= 1; --j) {
             udv_copy(Sj(j), Sj(j + 1), n);
             udv_record(ch, DQMC_UDV_STACK_SUFFIX_PRE_RMUL, min(j * stab, L), j, n, Sj(j).ell,
                        nullptr, s);
+            if (threadIdx.x == 0) ch->pcalls[DQMC_PH_STACK]++;   /* udv_rmul calls */
             udv_rmul(n, Sj(j), ch->bcache + j * nn, w, s, flag);
             if (*flag) return false;
         }
@@ -585,7 +588,7 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
 #endif
             wrap_green(n, G, tmp, md.expK, md.expKinv, fl, v0, v1, md.expvinv[0],
                        md.expvinv[1], s);
-        pc.charge(ch, DQMC_PH_WRAP);
+        pc.charge(ch, DQMC_PH_WRAP, 1);
         const bool boundary = ((l + 1) % stab == 0) && (l + 1 < L);
         const bool last = (l + 1 == L);
         if (!boundary && !last) continue;
@@ -603,17 +606,17 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
                     ch->sdrift_max_sweep = ch->sweeps;
                 }
             }
-            pc.charge(ch, DQMC_PH_SDRIFT);
+            pc.charge(ch, DQMC_PH_SDRIFT, 1);
         }
         const int te = boundary ? l + 1 : L;
         const int jblk = (boundary ? (l + 1) / stab : M) - 1;
         if (te > tau_left) {
             bblock(n, tau_left, te - tau_left, ch->field, md.expK, v0, v1,
                    ch->bcache + jblk * nn, tmp, tmp2, s);
-            pc.charge(ch, DQMC_PH_BBLOCK);
+            pc.charge(ch, DQMC_PH_BBLOCK, 1);
             udv_lmul(n, left, ch->bcache + jblk * nn, nullptr, nullptr, 0.0, 0.0, w, s, flag);
             if (*flag) return false;
-            pc.charge(ch, DQMC_PH_LMUL);
+            pc.charge(ch, DQMC_PH_LMUL, 1);
         }
         tau_left = te;
         if (alt) udv_copy(Pj(boundary ? (l + 1) / stab : M), left, n);   /* dqmc.c:704-706,767 */
@@ -628,12 +631,12 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         } else if (boundary) {
             udv_combine(n, left, Sj((l + 1) / stab), comb, w, s, flag);
             if (*flag) return false;
-            pc.charge(ch, DQMC_PH_COMBINE);
+            pc.charge(ch, DQMC_PH_COMBINE, 1);
             ds = udv_green(n, comb, Gn, w, s, flag);
         } else {
             ds = udv_green(n, left, Gn, w, s, flag);
         }
-        pc.charge(ch, DQMC_PH_GREEN);
+        pc.charge(ch, DQMC_PH_GREEN, 1);
         if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
         __syncthreads();
         if (*flag) return false;
@@ -650,7 +653,7 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
             if (d > ch->drift_max || ch->drift_count == 1) ch->drift_max = d;
             ch->sign = 1.0;
         }
-        pc.charge(ch, DQMC_PH_ADOPT);
+        pc.charge(ch, DQMC_PH_ADOPT, 1);
     }
     return true;
 }
@@ -676,6 +679,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     PhaseClock pc;
     pc.mark();
     if (!ch->pvalid) {
+        if (threadIdx.x == 0) ch->pcalls[DQMC_PH_BCACHE]++;
         /* green_stack_build_prefix (green.c:228-250) */
         udv_identity(Pj(0), n);
         for (int j = 1; j <= M; ++j) {
@@ -695,7 +699,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     auto back_wrap = [&](int l) {
         wrap_green_back(n, G, tmp, md.expK, md.expKinv, ch->field + (size_t)l * n, v0, v1,
                         md.expvinv[0], md.expvinv[1], s);
-        pc.charge(ch, DQMC_PH_WRAP);
+        pc.charge(ch, DQMC_PH_WRAP, 1);
     };
     auto rebuild = [&](int tau, Udv u, bool boundary, int j) {
         if (kflags & KF_SDRIFT) {
@@ -711,14 +715,14 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
                     ch->sdrift_max_sweep = ch->sweeps;
                 }
             }
-            pc.charge(ch, DQMC_PH_SDRIFT);
+            pc.charge(ch, DQMC_PH_SDRIFT, 1);
         }
         const int b1 = min(tau + stab, L);
         bblock(n, tau, b1 - tau, ch->field, md.expK, v0, v1, ch->bcache + j * nn, tmp, tmp2, s);
-        pc.charge(ch, DQMC_PH_BBLOCK);
+        pc.charge(ch, DQMC_PH_BBLOCK, 1);
         udv_rmul(n, u, ch->bcache + j * nn, w, s, flag);
         if (*flag) return false;
-        pc.charge(ch, DQMC_PH_LMUL);
+        pc.charge(ch, DQMC_PH_LMUL, 1);
         int ds;
         if (boundary) {
             udv_copy(Sj(j), u, n);
@@ -728,14 +732,14 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
             } else {
                 udv_combine(n, Pj(j), u, comb, w, s, flag);
                 if (*flag) return false;
-                pc.charge(ch, DQMC_PH_COMBINE);
+                pc.charge(ch, DQMC_PH_COMBINE, 1);
                 ds = udv_green(n, comb, Gn, w, s, flag);
             }
         } else {
             udv_record(ch, DQMC_UDV_LEFT_BACKWARD, 0, 0, n, u.ell, nullptr, s);   /* dqmc.c:926 */
             ds = udv_green(n, u, Gn, w, s, flag);
         }
-        pc.charge(ch, DQMC_PH_GREEN);
+        pc.charge(ch, DQMC_PH_GREEN, 1);
         if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
         __syncthreads();
         if (*flag) return false;
@@ -752,7 +756,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
             if (d > ch->drift_max || ch->drift_count == 1) ch->drift_max = d;
             ch->sign = 1.0;
         }
-        pc.charge(ch, DQMC_PH_ADOPT);
+        pc.charge(ch, DQMC_PH_ADOPT, 1);
         return true;
     };
     back_wrap(L - 1);
@@ -1013,7 +1017,7 @@ __global__ void __launch_bounds__(NT)
         }
     }
     __syncthreads();
-    pc.charge(ch, DQMC_PH_MEASURE);
+    pc.charge(ch, DQMC_PH_MEASURE, 1);
 }
 
 /* ---------------------------------------------------------- launchers */

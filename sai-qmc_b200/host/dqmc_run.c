@@ -129,8 +129,122 @@ static int write_q(FILE *fp, const DqmcSpinPlan *plan, double breq, double beta,
     return (fflush(fp) != 0 || ferror(fp)) ? 1 : 0;
 }
 
-static const char *phase_names[] = {"bcache", "stack", "propose", "flush", "wrap", "bblock",
-                                    "lmul", "combine", "green", "sdrift", "adopt", "measure"};
+static double now_s(void)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+/* ---- profile.dat (src/profiler.c) ----------------------------------------
+ * Regions and phases in the reference's order (src/profiler.c:10-29).  The
+ * sweep work is timed on the device: each chain's SM cycle counters and
+ * call counters (include/dqmc_gpu.h) become seconds at the SM clock and are
+ * summed over the beta's replicas like the reference's merged per-replica
+ * profilers (thread time; with many chains in flight frac_beta exceeds 1,
+ * as thread time does under OpenMP).  Device phases map onto regions:
+ * dqmc_sweep = every sweep phase, green_stack_build = B-block cache +
+ * stack, green_update = proposals + G updates (calls: accepted flips + G
+ * updates), green_wrap, udv_lmul (boundary UDV updates, rmuls of backward
+ * sweeps included), udv_rmul (suffix-stack rmuls), udv_combine, udv_inv_one_plus (G from UDV),
+ * green_from_stack (combine + G from UDV + adoption), green_from_scratch
+ * (reference drift rebuilds), measure_sample (the fused measurement,
+ * spin correlations included).  Setup regions are host wall time shared by
+ * the batch (model_init: the shared model's set-up, counted once per
+ * replica as the reference calls it; field_init and dqmc_init in proportion
+ * to the beta's chains), finalize = the beta's jackknife and outputs (one
+ * call); beta_total = the whole batched run up to this beta's outputs. */
+enum { R_BETA_TOTAL, R_MODEL_INIT, R_FIELD_INIT, R_DQMC_INIT, R_DQMC_SWEEP,
+       R_GREEN_FROM_SCRATCH, R_GREEN_WRAP, R_GREEN_UPDATE, R_MEASURE_SAMPLE, R_MEASURE_SZZ,
+       R_MEASURE_SPERP, R_MEASURE_SPIN, R_JACKKNIFE, R_UDV_LMUL, R_UDV_RMUL, R_UDV_COMBINE,
+       R_UDV_INV, R_STACK_BUILD, R_FROM_STACK, R_LA_GEMM, R_LA_INVERSE, R_LA_EXPM, R_COUNT };
+static const char *region_names[R_COUNT] = {
+    "beta_total", "model_init", "field_init", "dqmc_init", "dqmc_sweep", "green_from_scratch",
+    "green_wrap", "green_update", "measure_sample", "measure_szz", "measure_sperp",
+    "measure_spin", "jackknife", "udv_lmul", "udv_rmul", "udv_combine", "udv_inv_one_plus",
+    "green_stack_build", "green_from_stack", "la_gemm", "la_inverse", "la_expm_sym"};
+static const char *prof_phase_names[5] = {"setup", "warmup", "measurement", "finalize", "all"};
+
+typedef struct {
+    unsigned long long calls;
+    double sec;
+} PStat;
+
+typedef struct {
+    unsigned long long cy[12], ca[12], sweeps;
+} ProfSnap;
+
+/* counters of every chain, beta-major (b * nrep + r) */
+static int prof_snapshot(dqmc_engine **engs, int neng, int nrep, int nb, ProfSnap *out)
+{
+    if (!out) return 1;
+    for (int b = 0; b < nb; b++)
+        for (int r = 0; r < nrep; r++) {
+            const int k = dqmc_replica_rank_for_replica(nrep, neng, r);
+            int first, count;
+            dqmc_replica_rank_range(nrep, neng, k, &first, &count);
+            const int lc = b * count + (r - first);
+            ProfSnap *o = out + (size_t)b * nrep + r;
+            dqmc_chain_counters cnt;
+            if (dqmc_read_profile(engs[k], lc, o->cy, 12) ||
+                dqmc_read_profile_calls(engs[k], lc, o->ca, 12) ||
+                dqmc_read_counters(engs[k], lc, &cnt))
+                return 1;
+            o->sweeps = cnt.sweeps;
+        }
+    return 0;
+}
+
+static void padd(PStat *st, unsigned long long calls, double sec)
+{
+    st->calls += calls;
+    st->sec += sec;
+}
+
+/* regions of the device counters between two snapshots of one chain */
+static void prof_device(PStat *st, const ProfSnap *a, const ProfSnap *b, double hz)
+{
+    double sec[12];
+    unsigned long long ca[12];
+    for (int k = 0; k < 12; k++) {
+        sec[k] = (double)(b->cy[k] - (a ? a->cy[k] : 0)) / hz;
+        ca[k] = b->ca[k] - (a ? a->ca[k] : 0);
+    }
+    double sweep = 0.0;
+    for (int k = 0; k < 11; k++) sweep += sec[k];
+    padd(&st[R_DQMC_SWEEP], b->sweeps - (a ? a->sweeps : 0), sweep);
+    padd(&st[R_GREEN_FROM_SCRATCH], ca[9], sec[9]);
+    padd(&st[R_GREEN_WRAP], ca[4], sec[4]);
+    padd(&st[R_GREEN_UPDATE], ca[2] + ca[3], sec[2] + sec[3]);
+    padd(&st[R_MEASURE_SAMPLE], ca[11], sec[11]);
+    padd(&st[R_UDV_LMUL], ca[6], sec[6]);
+    padd(&st[R_UDV_RMUL], ca[1], sec[1]);
+    padd(&st[R_UDV_COMBINE], ca[7], sec[7]);
+    padd(&st[R_UDV_INV], ca[8], sec[8]);
+    padd(&st[R_STACK_BUILD], ca[0], sec[0] + sec[1]);
+    padd(&st[R_FROM_STACK], ca[10], sec[7] + sec[8] + sec[10]);
+}
+
+/* profiler_beta_end (src/profiler.c:188-223) */
+static void prof_rows(FILE *f, double beta, double T, double dtau, int Ltr, int nrep,
+                      const char *parallel, int nranks, PStat st[5][R_COUNT])
+{
+    for (int r = 0; r < R_COUNT; r++)
+        for (int ph = 0; ph < 4; ph++) padd(&st[4][r], st[ph][r].calls, st[ph][r].sec);
+    const double bt = st[4][R_BETA_TOTAL].sec;
+    for (int ph = 0; ph < 5; ph++)
+        for (int r = 0; r < R_COUNT; r++) {
+            const PStat x = st[ph][r];
+            if (x.calls == 0) continue;
+            fprintf(f, "%.17g %.17g %.17g %d %s %s %llu %.17g %.17g %.17g %.17g %.17g %d %s", beta,
+                    T, dtau, Ltr, prof_phase_names[ph], region_names[r], x.calls, x.sec,
+                    x.sec / (double)x.calls, bt > 0.0 ? x.sec / bt : 0.0,
+                    r == R_BETA_TOTAL ? bt : 0.0, x.sec, nrep, parallel);
+            if (nranks > 1) fprintf(f, " %d", nranks);
+            fprintf(f, "\n");
+        }
+    fflush(f);
+}
 
 static int udv_header(const char *path, const char *what, const char *header)
 {
@@ -314,6 +428,9 @@ int dqmc_host_run(const char *input)
     int neng = 1, devs[DQMC_MAX_GPUS];
     double *scal = NULL, *zz = NULL, *pp = NULL, *series = NULL, *zbins = NULL, *pbins = NULL;
     unsigned long long *seeds = NULL;
+    double tm[5] = {0, 0, 0, 0, 0};   /* model, field, init, warm-up, measurement walls */
+    ProfSnap *snap = NULL;
+    double t0s = 0.0;
     int *Ltrs = NULL;
     int shared = 0, cons = 0, write_rlog = 0, nb_ok = 0;
     const DqmcSpinPlan *sp = &pplan;
@@ -495,9 +612,11 @@ int dqmc_host_run(const char *input)
             fprintf(stderr, "ERROR: failed to initialize profiler output\n");
             goto out;
         }
-        fprintf(prof_fp, "# beta T dtau Ltr nrep wall_s");
-        for (int k = 0; k < 12; k++) fprintf(prof_fp, " %s_cycles", phase_names[k]);
-        fprintf(prof_fp, "\n");
+        /* profiler_init (src/profiler.c:56-76); the MPI build's header when
+         * the replicas are split over devices */
+        fprintf(prof_fp, "# beta T dtau Ltr phase region calls total_sec avg_sec frac_beta "
+                         "wall_sec thread_total_sec nrep parallel%s\n",
+                p.ngpu > 1 ? " nranks" : "");
     }
     /* betas run together; the first beta that is not a multiple of dtau
      * ends the run after the betas before it, as the reference does */
@@ -522,8 +641,7 @@ int dqmc_host_run(const char *input)
                     goto out;
                 }
     }
-    struct timespec t0, t1;
-    clock_gettime(CLOCK_MONOTONIC, &t0);
+    t0s = now_s();
     if (p.ngpu > 0) {
         neng = p.ngpu;
         for (int k = 0; k < neng; k++) devs[k] = p.gpu_devices[k];
@@ -555,6 +673,7 @@ int dqmc_host_run(const char *input)
                 fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
                 goto out;
             }
+            double ts = now_s();
             const int model =
                 dqmc_model_add(engs[k], L.n, L.has_coordinates ? L.Lx : 0,
                                L.has_coordinates ? L.Ly : 0, L.t, L.bipart, p.U, p.dtau);
@@ -564,6 +683,8 @@ int dqmc_host_run(const char *input)
                 fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
                 goto out;
             }
+            tm[0] += now_s() - ts;
+            ts = now_s();
             for (int b = 0; b < nb_ok; b++)
                 for (int r = first; r < first + count; r++)
                     if (dqmc_chain_add(engs[k], model, Ltrs[b], p.stab_interval,
@@ -571,13 +692,36 @@ int dqmc_host_run(const char *input)
                         fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
                         goto out;
                     }
+            tm[1] += now_s() - ts;
         }
         const int per = p.nmeas / nbin;
+        double ts = now_s();
         for (int k = 0; k < neng; k++)
-            if (engs[k] && (dqmc_engine_prepare(engs[k], nbin) || dqmc_sweep(engs[k], p.nwarm))) {
+            if (engs[k] && (dqmc_engine_prepare(engs[k], nbin) || dqmc_synchronize(engs[k]))) {
                 fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
                 goto out;
             }
+        tm[2] = now_s() - ts;
+        ts = now_s();
+        for (int k = 0; k < neng; k++)
+            if (engs[k] && dqmc_sweep(engs[k], p.nwarm)) {
+                fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                goto out;
+            }
+        if (prof_fp) {   /* profiler phase boundary (src/replica_run.c:183-200) */
+            for (int k = 0; k < neng; k++)
+                if (engs[k] && dqmc_synchronize(engs[k])) {
+                    fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                    goto out;
+                }
+            tm[3] = now_s() - ts;
+            if (prof_snapshot(engs, neng, nrep, nb_ok, snap = calloc((size_t)nb_ok * nrep * 2,
+                                                                        sizeof(ProfSnap)))) {
+                fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                goto out;
+            }
+            ts = now_s();
+        }
         for (int bi = 0; bi < nbin; bi++)
             for (int k = 0; k < neng; k++)
                 if (engs[k] && dqmc_sweep_measure(engs[k], per, bi)) {
@@ -589,9 +733,14 @@ int dqmc_host_run(const char *input)
                 fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
                 goto out;
             }
+        if (prof_fp) {
+            tm[4] = now_s() - ts;
+            if (prof_snapshot(engs, neng, nrep, nb_ok, snap + (size_t)nb_ok * nrep)) {
+                fprintf(stderr, "ERROR: %s\n", dqmc_last_error());
+                goto out;
+            }
+        }
     }
-    clock_gettime(CLOCK_MONOTONIC, &t1);
-    const double wall = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
     scal = malloc(sizeof(double) * (size_t)nbin * DQMC_BIN_NFIELDS);
     zz = malloc(sizeof(double) * (size_t)nbin * (zplan.nq + 1));
     pp = malloc(sizeof(double) * (size_t)nbin * (sp->nq + 1));
@@ -602,7 +751,7 @@ int dqmc_host_run(const char *input)
     for (int b = 0; b < nb_ok; b++) {
         const double beta = p.beta_list[b], beta_eff = Ltrs[b] * p.dtau, T = 1.0 / beta_eff;
         int any_failed = 0;
-        unsigned long long pcyc[12] = {0};
+        const double tfin = now_s();
         for (int r = 0; r < nrep; r++) {
             const int c = b * nrep + r;
             int lc;
@@ -634,11 +783,6 @@ int dqmc_host_run(const char *input)
             if ((p.udv_scale_file[0] || p.udv_centered_file[0]) &&
                 write_udv_records(&p, e, lc, b, Ltrs[b], r, seeds[c], L.n))
                 goto out;
-            if (prof_fp) {
-                unsigned long long cy[12];
-                dqmc_read_profile(e, lc, cy, 12);
-                for (int k = 0; k < 12; k++) pcyc[k] += cy[k];
-            }
         }
         if (replica_fp) {
             for (int r = 0; r < nrep; r++) {
@@ -733,9 +877,26 @@ int dqmc_host_run(const char *input)
             goto out;
         }
         if (prof_fp) {
-            fprintf(prof_fp, "%.17g %.17g %.17g %d %d %.6f", beta, T, p.dtau, Ltrs[b], nrep, wall);
-            for (int k = 0; k < 12; k++) fprintf(prof_fp, " %llu", pcyc[k]);
-            fprintf(prof_fp, "\n");
+            PStat st[5][R_COUNT];
+            memset(st, 0, sizeof st);
+            const double hz = dqmc_clock_hz(engs[dqmc_replica_rank_for_replica(nrep, neng, 0)]);
+            const double share = (double)nrep / (double)(nrep * nb_ok);
+            padd(&st[0][R_MODEL_INIT], nrep, tm[0]);   /* one model_init per replica */
+            padd(&st[0][R_FIELD_INIT], nrep, tm[1] * share);
+            padd(&st[0][R_DQMC_INIT], nrep, tm[2] * share);
+            for (int r = 0; r < nrep; r++) {
+                const ProfSnap *w = snap + (size_t)b * nrep + r;
+                const ProfSnap *m = snap + (size_t)(nb_ok + b) * nrep + r;
+                if (hz > 0) {
+                    prof_device(st[1], NULL, w, hz);
+                    prof_device(st[2], w, m, hz);
+                }
+            }
+            const double tend = now_s();
+            padd(&st[3][R_JACKKNIFE], 1, tend - tfin);   /* one finalize per beta */
+            st[4][R_BETA_TOTAL].calls = 1;
+            st[4][R_BETA_TOTAL].sec = (tfin - t0s) + (tend - tfin);
+            prof_rows(prof_fp, beta, T, p.dtau, Ltrs[b], nrep, p.parallel, neng, st);
         }
     }
     if (nb_ok < p.nbeta) {
@@ -765,5 +926,6 @@ out:
     free(pbins);
     free(seeds);
     free(Ltrs);
+    free(snap);
     return rc;
 }

@@ -157,3 +157,56 @@ def test_cli_replicas_split_over_devices(tmp_path):
     for x, y in zip(ra, rb):
         assert len(x) == 8 and len(y) == 9 and x == y[:8]
         assert int(y[8]) == (0 if int(y[2]) < 2 else 1)
+
+
+def prof_table(path):
+    out = {}
+    for l in open(path):
+        if l.startswith("#"):
+            continue
+        x = l.split()
+        assert len(x) == 14
+        out[(x[0], x[4], x[5])] = (int(x[6]), float(x[7]), float(x[9]))
+    return out
+
+
+def test_cli_profile_file_like_reference(tmp_path):
+    """profile=1: the reference's profile.dat rows (src/profiler.c:188-223).
+    Region call counts that are fixed by the algorithm equal the reference
+    program's; times are the engine's own (device cycles at the SM clock)."""
+    g = tmp_path / "gpu"
+    g.mkdir()
+    run(EXE, g, "profile=1\n")
+    head = open(g / "profile.dat").readline()
+    assert head == ("# beta T dtau Ltr phase region calls total_sec avg_sec frac_beta wall_sec "
+                    "thread_total_sec nrep parallel\n")
+    t = prof_table(g / "profile.dat")
+    betas = sorted({k[0] for k in t})
+    assert len(betas) == 3
+    for b in betas:
+        bt = t[(b, "all", "beta_total")]
+        assert bt[0] == 1 and bt[1] > 0
+        for ph in ("warmup", "measurement"):
+            assert t[(b, ph, "dqmc_sweep")][0] == 2 * (20 if ph == "warmup" else 40)
+        for (bb, ph, reg), (calls, sec, frac) in t.items():
+            if bb != b or reg == "beta_total":
+                continue
+            assert calls > 0 and sec >= 0 and abs(frac - sec / bt[1]) <= 1e-12 * max(1, frac)
+            if ph == "all":
+                parts = [t.get((b, p, reg), (0, 0.0, 0))[0]
+                         for p in ("setup", "warmup", "measurement", "finalize")]
+                assert calls == sum(parts)
+    if os.path.exists(REF_EXE):
+        r = tmp_path / "ref"
+        r.mkdir()
+        run(REF_EXE, r, "profile=1\n")
+        assert open(r / "profile.dat").readline() == head
+        ref = prof_table(r / "profile.dat")
+        fixed = ("dqmc_sweep", "green_wrap", "measure_sample", "green_stack_build", "udv_lmul",
+                 "udv_rmul", "udv_combine", "udv_inv_one_plus")
+        n = 0
+        for (b, ph, reg), v in ref.items():
+            if ph in ("warmup", "measurement") and reg in fixed:
+                assert t[(b, ph, reg)][0] == v[0], (b, ph, reg)
+                n += 1
+        assert n > 0
