@@ -64,6 +64,7 @@ enum {
     DQMC_UDV_R_LEFT = 4,    /* min, max, finite, zero, nonfinite of the (left) factor */
     DQMC_UDV_R_RIGHT = 9,   /* the same for the right factor of a boundary pair      */
     DQMC_UDV_R_HAS_RIGHT = 14,
+    DQMC_UDV_R_SPIN = 15,   /* 0: G_up ("u"), 1: G_down ("d") of the two-spin path */
     DQMC_UDV_RECORD_DOUBLES = 16
 };
 
@@ -135,6 +136,19 @@ const char *dqmc_last_error(void);
  * Returns the model id (>= 0) or -1. */
 int dqmc_model_add(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
                    const int *bipart, double U, double dtau);
+/* dqmc_model_add with a chemical potential (model_init, src/model.c:8-31):
+ * half_filling = 1 sets mu = U/2 (mu ignored), else K = t - mu I.  Chains of
+ * a model that is not particle-hole symmetric -- not at half filling, or
+ * bipart NULL for a non-bipartite lattice -- evolve G_up and G_down
+ * separately (the reference's use_ph = 0 path, src/dqmc.c:418-483,
+ * 641-813): joint acceptance R = R_up R_down, a running sign reset to
+ * det_up * det_down at every stabilization.  two_spin = 1 takes that path
+ * also at the PH point (the reference's ph_symmetric = 0 override in
+ * tests/test_dqmc_stack.c:81).  The two-spin path runs forward sweeps in
+ * FP64, one chain per SM.  Returns the model id or -1. */
+int dqmc_model_add_mu(dqmc_engine *e, int n, int Lx, int Ly, const double *t,
+                      const int *bipart, double U, double dtau, int half_filling,
+                      double mu, int two_spin);
 
 /* Enables Szz(q) / Sperp(q) on a model for the q lists (mx, my), the
  * structure_factor_plan_init selectors of src/structure_factor.c:107-206.
@@ -187,6 +201,9 @@ int dqmc_chain_dims(const dqmc_engine *e, int chain, int *n, int *L);
 /* Copies back the up-spin G (n x n) at the chain's current slice (0 after a
  * sweep).  G_down = I - P G_up^T P (src/green.c:372-382). */
 int dqmc_read_green(dqmc_engine *e, int chain, double *G);
+/* G_down of a chain: the evolved matrix on the two-spin path, else the PH
+ * map of G_up (dqmc_map_ph_down, src/dqmc.c:9-17). */
+int dqmc_read_green_down(dqmc_engine *e, int chain, double *G);
 int dqmc_read_field(dqmc_engine *e, int chain, signed char *field);
 /* Replaces a chain's field and rebuilds its G from scratch. */
 int dqmc_write_field(dqmc_engine *e, int chain, const signed char *field);

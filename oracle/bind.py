@@ -231,6 +231,20 @@ class Reference:
         lib.ref_rng_first.argtypes = [C.c_ulonglong, C.c_int, _dp]
         self.lib = lib
 
+    def chain_mu(self, kind, Lx, Ly, U, dtau, L, stab, seed, half=True, mu=0.0,
+                 two_spin=False, pbc=1, t=-1.0):
+        """A reference chain on model_init(half, mu), optionally forced onto
+        its two-spin path (ph_symmetric = 0)."""
+        n = Lx * (Ly if kind == LAT_SQUARE else 1)
+        self.lib.ref_chain_new_mu.restype = C.c_void_p
+        self.lib.ref_chain_new_mu.argtypes = [C.c_int] * 4 + [C.c_double] * 3 + \
+            [C.c_int, C.c_int, C.c_ulonglong, C.c_int, C.c_double, C.c_int]
+        h = self.lib.ref_chain_new_mu(kind, Lx, Ly, pbc, t, U, dtau, L, stab, seed, int(half),
+                                      mu, int(two_spin))
+        ch = _Chain(self.lib, "ref_", h, n, L)
+        ch.kind, ch.Lx, ch.Ly = kind, Lx, (Ly if kind == LAT_SQUARE else 1)
+        return ch
+
     def chain(self, kind, Lx, Ly, U, dtau, L, stab, seed, field=None,
               pbc=1, t=-1.0, drift=False, alternating=False, rebuild=0):
         n = Lx * (Ly if kind == LAT_SQUARE else 1)

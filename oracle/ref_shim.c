@@ -13,6 +13,9 @@
  *                      field_init (field.c:6-24), dqmc_init_modes
  *                      (dqmc.c:418-483)
  *   ref_chain_new_mode the same with sweep_order and green_rebuild
+ *   ref_chain_new_mu   the same with model_init's half/mu arguments and the
+ *                      ph_symmetric = 0 override of tests/test_dqmc_stack.c:81
+ *                      (the reference's two-spin path, dqmc.c:418-483)
  *   ref_chain_sweep    dqmc_sweep (dqmc.c:952-963)
  *   ref_chain_measure  measure_sample (measure.c:6-39) and
  *                      measure_szz_sperp_sample (structure_factor.c:328-400)
@@ -90,6 +93,33 @@ void *ref_chain_new_mode(int kind, int Lx, int Ly, int pbc, double t, double U,
     if (enable_drift) {
         dqmc_enable_stab_drift(&c->D, 1);
     }
+    return c;
+}
+
+/* As ref_chain_new on a model_init(half, mu) model; force_two_spin sets
+ * ph_symmetric = 0 before dqmc_init so the two-spin path runs even at the
+ * particle-hole point. */
+void *ref_chain_new_mu(int kind, int Lx, int Ly, int pbc, double t, double U, double dtau,
+                       int L, int stab, unsigned long long seed, int half, double mu,
+                       int force_two_spin)
+{
+    RefChain *c = calloc(1, sizeof(RefChain));
+    if (c == NULL) {
+        return NULL;
+    }
+    if (kind == 0) {
+        lattice_chain(&c->lat, Lx, t, pbc);
+    } else {
+        lattice_square(&c->lat, Lx, Ly, t, pbc);
+    }
+    model_init(&c->m, &c->lat, U, dtau, half, mu);
+    if (force_two_spin) {
+        c->m.ph_symmetric = 0;
+    }
+    rng_seed(&c->r, seed);
+    field_init(&c->f, c->lat.n, L, U, dtau, &c->r);
+    c->stab = stab;
+    dqmc_init(&c->D, &c->m, &c->f, &c->r, stab, NULL);
     return c;
 }
 

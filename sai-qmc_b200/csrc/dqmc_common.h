@@ -58,6 +58,9 @@ typedef struct {
     double U, dtau, mu;
     double expv[2];     /* exp(+lambda*s - dtau*U/2) for s = -1, +1 (green.c:63-67) */
     double expvinv[2];  /* 1/expv                                           */
+    /* the same for sigma = -1 (G_down of the two-spin path, green.c:63-67) */
+    double expvd[2], expvinvd[2];
+    int ph;             /* 1: particle-hole path (G_down mapped from G_up)  */
     double Nup[2];      /* N_cache[sigma=+1][s] = exp(-2 lambda s) - 1 (field.c:11-17) */
     double Ndn[2];      /* N_cache[sigma=-1][s] = exp(+2 lambda s) - 1      */
     const double *expK, *expKinv, *thop;
@@ -81,6 +84,7 @@ typedef struct {
     int alt, dir, pvalid, svalid;
     int rebuild;               /* 0: combine, 1: two-sided G at boundaries */
     int pair;                  /* flush G after every second site block   */
+    int ns;                    /* evolved spins: 1 (PH path) or 2 (G_up, G_down) */
     /* UDV scale records (opt-in): DQMC_UDV_RECORD_DOUBLES each, udv_n of
      * udv_cap used since the host last drained them, udv_lost dropped */
     int udv_cap, udv_n, udv_lost;
@@ -105,6 +109,8 @@ typedef struct {
     double *bcache;            /* M x n x n block products B(b_{j+1}, b_j) */
     double *w[6];              /* n x n scratch */
     double *Zs, *Ys;           /* n x 2kb / 2kb x n flush operands (two blocks) */
+    /* G_down's own state on the two-spin path (else null) */
+    double *Gd, *Sd, *leftd, *combd, *bcached, *Zsd, *Ysd;
     double *twall;             /* n x QNB compact-WY factors of the last QR */
     double *bins;              /* nbin x DQMC_BIN_FIELDS */
     double *bins_zz, *bins_perp;   /* nbin x nq */

@@ -116,6 +116,8 @@ size_t rup(size_t b) { return (b + 255) & ~(size_t)255; }
 struct HModel {
     int n, Lx, Ly;
     double U, dtau;
+    double mu = 0.0;
+    int ph = 1;   /* particle-hole path (half filling on a bipartite lattice) */
     std::vector<double> thop, expK, expKinv, cos_zz, cos_perp;
     std::vector<int> bipart;
     int nq_zz = 0, nq_perp = 0;
@@ -276,10 +278,19 @@ void dqmc_engine_destroy(dqmc_engine *e)
 int dqmc_model_add(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
                    const int *bipart, double U, double dtau)
 {
+    if (!bipart) return -set_err("dqmc_model_add: null bipart (see dqmc_model_add_mu)");
+    return dqmc_model_add_mu(e, n, Lx, Ly, thop, bipart, U, dtau, 1, 0.0, 0);
+}
+
+int dqmc_model_add_mu(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
+                      const int *bipart, double U, double dtau, int half_filling, double mu,
+                      int two_spin)
+{
     if (!e || e->prepared) return -set_err("dqmc_model_add: engine missing or prepared");
-    if (n <= 0 || n > DQMC_MAX_N || !thop || !bipart)
+    if (n <= 0 || n > DQMC_MAX_N || !thop)
         return -set_err("dqmc_model_add: n=%d outside 1..%d or null input", n, DQMC_MAX_N);
     if (!(dtau > 0.0) || !(U >= 0.0)) return -set_err("dqmc_model_add: need U>=0, dtau>0");
+    if (!half_filling && !std::isfinite(mu)) return -set_err("dqmc_model_add: mu not finite");
     HModel m;
     m.n = n;
     m.Lx = Lx;
@@ -287,10 +298,14 @@ int dqmc_model_add(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
     m.U = U;
     m.dtau = dtau;
     m.thop.assign(thop, thop + (size_t)n * n);
-    m.bipart.assign(bipart, bipart + n);
-    /* model_init (src/model.c:8-31): K = t - mu I with mu = U/2 */
+    if (bipart) m.bipart.assign(bipart, bipart + n);
+    else m.bipart.assign(n, 0);
+    /* model_init (src/model.c:8-31): mu = U/2 at half filling, K = t - mu I;
+     * the PH path needs half filling on a bipartite lattice (ph_symmetric) */
+    m.mu = half_filling ? U / 2.0 : mu;
+    m.ph = (half_filling && bipart && !two_spin) ? 1 : 0;
     std::vector<double> K(m.thop);
-    for (int i = 0; i < n; ++i) K[i + (size_t)i * n] -= U / 2.0;
+    for (int i = 0; i < n; ++i) K[i + (size_t)i * n] -= m.mu;
     m.expK.resize((size_t)n * n);
     m.expKinv.resize((size_t)n * n);
     dqmc_expm_sym(n, K.data(), -dtau, m.expK.data());
@@ -398,6 +413,16 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     /* models */
     const bool mixed = e->desc.precision == DQMC_PREC_MIXED;
     const bool alt = e->desc.sweep_order == DQMC_SWEEP_ALTERNATING;
+    for (const HChain &c : e->chains) {
+        if (e->models[c.model].ph) continue;
+        /* dqmc_init_modes rejects the alternating order off the PH path
+         * (src/dqmc.c:440-446) */
+        if (alt)
+            return set_err("dqmc_engine_prepare: sweep_order=alternating needs the "
+                           "particle-hole path (half filling, bipartite lattice)");
+        if (mixed)
+            return set_err("dqmc_engine_prepare: precision=mixed needs the particle-hole path");
+    }
     if (mixed) {
         for (const HModel &m : e->models)
             if (!dq::qr_cb(m.n))
@@ -435,14 +460,20 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         d.Ly = m.Ly;
         d.U = m.U;
         d.dtau = m.dtau;
-        d.mu = m.U / 2.0;
-        /* field.c:10-17, green.c:63-67 (sigma = +1 for the evolved spin) */
+        d.mu = m.mu;
+        d.ph = m.ph;
+        /* field.c:10-17, green.c:63-67 (sigma = +1 for the evolved spin,
+         * -1 for G_down of the two-spin path) */
         const double lambda = std::acosh(std::exp(m.dtau * m.U / 2.0));
         const double c = -m.dtau * m.U / 2.0;
         d.expv[0] = std::exp(lambda * -1.0 + c);
         d.expv[1] = std::exp(lambda * 1.0 + c);
         d.expvinv[0] = 1.0 / d.expv[0];
         d.expvinv[1] = 1.0 / d.expv[1];
+        d.expvd[0] = std::exp(lambda * 1.0 + c);
+        d.expvd[1] = std::exp(lambda * -1.0 + c);
+        d.expvinvd[0] = 1.0 / d.expvd[0];
+        d.expvinvd[1] = 1.0 / d.expvd[1];
         for (int is = 0; is < 2; ++is) {
             const double sv = is ? 1.0 : -1.0;
             d.Nup[is] = std::exp(-2.0 * lambda * 1.0 * sv) - 1.0;
@@ -511,7 +542,11 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += 6 * rup(nn * 8);                               /* w */
         off += 2 * rup((size_t)n * 2 * c.kb * 8);             /* Zs, Ys */
         if (e->desc.udv_diag)                                  /* UDV scale records */
-            off += rup((size_t)udv_cap(c.M) * DQMC_UDV_RECORD_DOUBLES * 8);
+            off += rup((size_t)(m.ph ? 1 : 2) * udv_cap(c.M) * DQMC_UDV_RECORD_DOUBLES * 8);
+        if (!m.ph) {   /* G_down's state on the two-spin path */
+            off += rup(nn * 8) + rup((size_t)(c.M + 1) * usz * 8) + 2 * rup(usz * 8) +
+                   rup((size_t)c.M * nn * 8) + 2 * rup((size_t)n * 2 * c.kb * 8);
+        }
         off += rup((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB * DQMC_QNB * 8);
         off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
@@ -564,8 +599,19 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         d.Zs = (double *)take((size_t)n * 2 * c.kb * 8);
         d.Ys = (double *)take((size_t)n * 2 * c.kb * 8);
         if (e->desc.udv_diag) {
-            d.udv_cap = udv_cap(c.M);
+            d.udv_cap = (m.ph ? 1 : 2) * udv_cap(c.M);
             d.udvrec = (double *)take((size_t)d.udv_cap * DQMC_UDV_RECORD_DOUBLES * 8);
+        }
+        d.ns = m.ph ? 1 : 2;
+        if (!m.ph) {
+            d.pair = 0;
+            d.Gd = (double *)take(nn * 8);
+            d.Sd = (double *)take((size_t)(c.M + 1) * usz * 8);
+            d.leftd = (double *)take(usz * 8);
+            d.combd = (double *)take(usz * 8);
+            d.bcached = (double *)take((size_t)c.M * nn * 8);
+            d.Zsd = (double *)take((size_t)n * 2 * c.kb * 8);
+            d.Ysd = (double *)take((size_t)n * 2 * c.kb * 8);
         }
         d.twall = (double *)take((size_t)((n + DQMC_QNB - 1) / DQMC_QNB) * DQMC_QNB *
                                  DQMC_QNB * 8);
@@ -594,7 +640,12 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         const bool fits2 = 2 * (e->smem2 + 1024) <= 228 * 1024;
         const int want = e->desc.ctas_per_sm;
-        e->per_sm = (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 && !mixed ? 2 : 1;
+        /* the two-spin proposals hold both spins' block columns in
+         * registers: one CTA per SM */
+        bool two = false;
+        for (const HChain &c : e->chains) two = two || !e->models[c.model].ph;
+        e->per_sm =
+            (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 && !mixed && !two ? 2 : 1;
         if (e->per_sm == 2) CU(dq2x::set_attrs(e->smem2, e->msmem));
     }
     dq::k_init<<<(unsigned)nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels);
@@ -791,6 +842,26 @@ int dqmc_read_green(dqmc_engine *e, int chain, double *G)
     const int n = e->hdev[chain].n;
     CU(cudaStreamSynchronize(e->stream));
     CU(cudaMemcpy(G, e->hdev[chain].G, (size_t)n * n * 8, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int dqmc_read_green_down(dqmc_engine *e, int chain, double *G)
+{
+    if (chain_ok(e, chain, "dqmc_read_green_down")) return 1;
+    const DqmcChainDev &d = e->hdev[chain];
+    const int n = d.n;
+    CU(cudaStreamSynchronize(e->stream));
+    if (d.ns == 2) {
+        CU(cudaMemcpy(G, d.Gd, (size_t)n * n * 8, cudaMemcpyDeviceToHost));
+        return 0;
+    }
+    /* PH path: G_down = I - P G_up^T P (dqmc_map_ph_down, src/dqmc.c:9-17) */
+    std::vector<double> gu((size_t)n * n);
+    CU(cudaMemcpy(gu.data(), d.G, gu.size() * 8, cudaMemcpyDeviceToHost));
+    const std::vector<int> &p = e->models[e->chains[chain].model].bipart;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+            G[i + (size_t)j * n] = (i == j ? 1.0 : 0.0) - (double)(p[i] * p[j]) * gu[j + (size_t)i * n];
     return 0;
 }
 

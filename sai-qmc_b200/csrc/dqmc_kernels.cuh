@@ -58,115 +58,25 @@ __device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
  * Zs and Ys are formed one row / one column per thread (FP64 FMAs on the
  * accepted columns / rows of G, coalesced across the CTA): no CTA-wide GEMM
  * pipeline for these thin products. */
-__device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G,
-                                       signed char *fl, const DqmcModelDev &md,
-                                       uint64_t *rng, unsigned long long *att,
-                                       unsigned long long *acc, double *Zs, double *Ys,
-                                       int mA, bool flush, Smem &s, DqmcChainDev *ch,
-                                       PhaseClock &pc)
+/* The flush of one spin's site block after the proposals: the inverses Tu,
+ * Tv from the recorded rows / columns, Zs and Ys (with the staged block's
+ * corrections when mA > 0), and the G update when `flush`.  Rrow, Ccol,
+ * facs: that spin's records; TuP: where Tu is laid out with even rows (the
+ * spin's own Rrow area, free once the inverses exist).  Returns the staged
+ * count left for the next block (0 after a G update). */
+__device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G, double *Zs,
+                                        double *Ys, int mA, bool flush, double *Rrow,
+                                        double *Ccol, double *facs, double *TuP, Smem &s,
+                                        DqmcChainDev *ch, PhaseClock &pc)
 {
-    constexpr int KB = DQMC_MAX_KB;   /* 32: one lane per block column */
+    constexpr int KB = DQMC_MAX_KB;
     constexpr int LD = KB + 1;
-    constexpr int LT = KB + 2;        /* even rows: 16-byte pair loads  */
-    static_assert(GEMM_SMEM >= 3 * KB * LT && GEMM_SMEM % 2 == 0, "site-block staging");
+    constexpr int LT = KB + 2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double *Rrow = s.g0;              /* [q*LD + b] = G~_q[a_q, b]      */
-    double *Ccol = Rrow + KB * LD;    /* [q*LD + c] = G~_q[c, a_q]      */
-    double *Tu = Ccol + KB * LD;      /* (I - F Su)^-1, row-major [q*LD+p] */
-    double *Tv = Tu + KB * LD;        /* (I + Sc)^-1                     */
-    double *facs = Tv + KB * LD;      /* fac_q                           */
-    /* GEMM staging area, idle until the final flush: the staged block's
-     * entries at this block ZA[a][k] = Zs_A[i0+a, k], YA[k][b] = Ys_A[k,
-     * i0+b] (row length LD), later -Pa^T and Qa (row length LT); TvP. */
+    double *Tu = s.g0 + 2 * KB * LD, *Tv = Tu + KB * LD;
     double *ZA = s.gsm, *YA = s.gsm + KB * LT, *TvP = s.gsm + 2 * KB * LT;
-    double *TuP = Rrow;               /* Tu with row length LT, after the inverses */
-    int *alist = s.iscr;              /* accepted block positions, in order */
+    const int *alist = s.iscr;
     const int ldy = 2 * kb;
-    if (mA > 0) {
-        for (int e = tid; e < KB * KB; e += NT) {
-            const int a = e % KB, k = e / KB;
-            if (k < mA) ZA[a * LD + k] = a < kbs ? Zs[(i0 + a) + (size_t)k * n] : 0.0;
-            const int k2 = e % KB, b = e / KB;
-            if (k2 < mA) YA[k2 * LD + b] = b < kbs ? Ys[k2 + (size_t)(i0 + b) * ldy] : 0.0;
-        }
-        __syncthreads();
-        /* G~[B,B] = G[B,B] - ZA YA, row-major in the Tu area */
-        for (int e = tid; e < KB * KB; e += NT) {
-            const int c = e % KB, b = e / KB;
-            if (c < kbs && b < kbs) {
-                double v = G[(i0 + c) + (size_t)(i0 + b) * n];
-                for (int k = 0; k < mA; ++k) v = fma(-ZA[c * LD + k], YA[k * LD + b], v);
-                Tu[c * LD + b] = v;
-            }
-        }
-        __syncthreads();
-    }
-    if (warp == 0) {
-        double col[KB];
-        const bool mine = lane < kbs;
-#pragma unroll
-        for (int c = 0; c < KB; ++c)
-            col[c] = (mine && c < kbs) ? (mA > 0 ? Tu[c * LD + lane]
-                                                 : G[(i0 + c) + (size_t)(i0 + lane) * n])
-                                       : 0.0;
-        int fvl = mine ? (int)fl[i0 + lane] : 1;
-        const double Nu0 = md.Nup[0], Nu1 = md.Nup[1], Nd0 = md.Ndn[0], Nd1 = md.Ndn[1];
-        uint64_t r4[4] = {0, 0, 0, 0};
-        if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) r4[q] = rng[q];
-        }
-        unsigned long long nacc = 0;
-        int m = 0;
-#pragma unroll
-        for (int a = 0; a < KB; ++a) {
-            if (a < kbs) {
-                const int sv = __shfl_sync(FULL, fvl, a);
-                const double gii = __shfl_sync(FULL, col[a], a);
-                const bool up = sv > 0;
-                const double Nu = up ? Nu1 : Nu0, Nd = up ? Nd1 : Nd0;
-                const double Ru = 1.0 + (1.0 - gii) * Nu;
-                const double Rd = 1.0 + gii * Nd;
-                const double R = Ru * Rd;
-                double u = 0.0;
-                if (lane == 0) u = rng_next(r4);
-                u = __shfl_sync(FULL, u, 0);
-                if (u < fabs(R)) {
-                    const double fac = Nu / Ru;
-                    const double ra = col[a];        /* G~[a, lane] */
-                    double mycol = 0.0;              /* G~[lane, a] */
-                    const double fra = fac * ra;
-#pragma unroll
-                    for (int c = a + 1; c < KB; ++c) {
-                        const double vc = __shfl_sync(FULL, col[c], a);
-                        if (c == lane) mycol = vc;
-                        col[c] = fma(vc, fra, col[c]);
-                    }
-                    Rrow[m * LD + lane] = ra;
-                    Ccol[m * LD + lane] = mycol;
-                    if (lane == a) fvl = -sv;
-                    if (lane == 0) {
-                        facs[m] = fac;
-                        alist[m] = a;
-                        ++nacc;
-                    }
-                    ++m;
-                }
-            }
-        }
-        if (mine) fl[i0 + lane] = (signed char)fvl;
-        if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) rng[q] = r4[q];
-            *att += (unsigned long long)kbs;
-            *acc += nacc;
-            ch->pcalls[DQMC_PH_PROPOSE] += nacc;   /* green_delay_accept calls */
-            s.iscr[2 * DQMC_MAX_KB] = m;
-        }
-    }
-    __syncthreads();
-    pc.charge(ch, DQMC_PH_PROPOSE);
-    const int m = s.iscr[2 * DQMC_MAX_KB];
     if (m == 0) {
         if (!flush || mA == 0) return mA;
         gemm_nn_rmw(
@@ -387,6 +297,155 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
     return 0;
 }
 
+template <int NS>
+__device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G,
+                                       signed char *fl, const DqmcModelDev &md,
+                                       uint64_t *rng, unsigned long long *att,
+                                       unsigned long long *acc, double *Zs, double *Ys,
+                                       int mA, bool flush, Smem &s, DqmcChainDev *ch,
+                                       PhaseClock &pc, double *Gd = nullptr,
+                                       double *Zsd = nullptr, double *Ysd = nullptr)
+{
+    constexpr int KB = DQMC_MAX_KB;   /* 32: one lane per block column */
+    constexpr int LD = KB + 1;
+    constexpr int LT = KB + 2;        /* even rows: 16-byte pair loads  */
+    static_assert(GEMM_SMEM >= 3 * KB * LT && GEMM_SMEM % 2 == 0, "site-block staging");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double *Rrow = s.g0;              /* [q*LD + b] = G~_q[a_q, b]      */
+    double *Ccol = Rrow + KB * LD;    /* [q*LD + c] = G~_q[c, a_q]      */
+    double *Tu = Ccol + KB * LD;      /* (I - F Su)^-1, row-major [q*LD+p] */
+    double *Tv = Tu + KB * LD;        /* (I + Sc)^-1                     */
+    double *facs = Tv + KB * LD;      /* fac_q                           */
+    /* GEMM staging area, idle until the final flush: the staged block's
+     * entries at this block ZA[a][k] = Zs_A[i0+a, k], YA[k][b] = Ys_A[k,
+     * i0+b] (row length LD), later -Pa^T and Qa (row length LT); TvP. */
+    double *ZA = s.gsm, *YA = s.gsm + KB * LT, *TvP = s.gsm + 2 * KB * LT;
+    double *TuP = Rrow;               /* Tu with row length LT, after the inverses */
+    int *alist = s.iscr;              /* accepted block positions, in order */
+    /* two-spin path: G_down's records in the GEMM staging area (pairing is
+     * off there, and the down spin is flushed first) */
+    double *RrowD = s.gsm, *CcolD = RrowD + KB * LD, *facsD = CcolD + KB * LD;
+    const int ldy = 2 * kb;
+    if (mA > 0) {
+        for (int e = tid; e < KB * KB; e += NT) {
+            const int a = e % KB, k = e / KB;
+            if (k < mA) ZA[a * LD + k] = a < kbs ? Zs[(i0 + a) + (size_t)k * n] : 0.0;
+            const int k2 = e % KB, b = e / KB;
+            if (k2 < mA) YA[k2 * LD + b] = b < kbs ? Ys[k2 + (size_t)(i0 + b) * ldy] : 0.0;
+        }
+        __syncthreads();
+        /* G~[B,B] = G[B,B] - ZA YA, row-major in the Tu area */
+        for (int e = tid; e < KB * KB; e += NT) {
+            const int c = e % KB, b = e / KB;
+            if (c < kbs && b < kbs) {
+                double v = G[(i0 + c) + (size_t)(i0 + b) * n];
+                for (int k = 0; k < mA; ++k) v = fma(-ZA[c * LD + k], YA[k * LD + b], v);
+                Tu[c * LD + b] = v;
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        double col[KB], cold[NS == 2 ? KB : 1];
+        const bool mine = lane < kbs;
+#pragma unroll
+        for (int c = 0; c < KB; ++c)
+            col[c] = (mine && c < kbs) ? (mA > 0 ? Tu[c * LD + lane]
+                                                 : G[(i0 + c) + (size_t)(i0 + lane) * n])
+                                       : 0.0;
+        if constexpr (NS == 2) {
+#pragma unroll
+            for (int c = 0; c < KB; ++c)
+                cold[c] = (mine && c < kbs) ? Gd[(i0 + c) + (size_t)(i0 + lane) * n] : 0.0;
+        }
+        int neg = 0;   /* accepted flips with R < 0 (dqmc.c:672-674) */
+        int fvl = mine ? (int)fl[i0 + lane] : 1;
+        const double Nu0 = md.Nup[0], Nu1 = md.Nup[1], Nd0 = md.Ndn[0], Nd1 = md.Ndn[1];
+        uint64_t r4[4] = {0, 0, 0, 0};
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r4[q] = rng[q];
+        }
+        unsigned long long nacc = 0;
+        int m = 0;
+#pragma unroll
+        for (int a = 0; a < KB; ++a) {
+            if (a < kbs) {
+                const int sv = __shfl_sync(FULL, fvl, a);
+                const double gii = __shfl_sync(FULL, col[a], a);
+                const bool up = sv > 0;
+                const double Nu = up ? Nu1 : Nu0, Nd = up ? Nd1 : Nd0;
+                const double Ru = 1.0 + (1.0 - gii) * Nu;
+                /* green_ph_down_ratio_N, or green_delay_ratio_N on G_down
+                 * (green.c:402-416) */
+                double giid = 0.0;
+                if constexpr (NS == 2) giid = __shfl_sync(FULL, cold[a], a);
+                const double Rd = NS == 2 ? 1.0 + (1.0 - giid) * Nd : 1.0 + gii * Nd;
+                const double R = Ru * Rd;
+                double u = 0.0;
+                if (lane == 0) u = rng_next(r4);
+                u = __shfl_sync(FULL, u, 0);
+                if (u < fabs(R)) {
+                    const double fac = Nu / Ru;
+                    const double ra = col[a];        /* G~[a, lane] */
+                    double mycol = 0.0;              /* G~[lane, a] */
+                    const double fra = fac * ra;
+#pragma unroll
+                    for (int c = a + 1; c < KB; ++c) {
+                        const double vc = __shfl_sync(FULL, col[c], a);
+                        if (c == lane) mycol = vc;
+                        col[c] = fma(vc, fra, col[c]);
+                    }
+                    Rrow[m * LD + lane] = ra;
+                    Ccol[m * LD + lane] = mycol;
+                    if constexpr (NS == 2) {
+                        const double facd = Nd / Rd;
+                        const double rad = cold[a];
+                        double mycold = 0.0;
+                        const double frad = facd * rad;
+#pragma unroll
+                        for (int c = a + 1; c < KB; ++c) {
+                            const double vc = __shfl_sync(FULL, cold[c], a);
+                            if (c == lane) mycold = vc;
+                            cold[c] = fma(vc, frad, cold[c]);
+                        }
+                        RrowD[m * LD + lane] = rad;
+                        CcolD[m * LD + lane] = mycold;
+                        if (lane == 0) facsD[m] = facd;
+                        if (R < 0.0) neg ^= 1;
+                    }
+                    if (lane == a) fvl = -sv;
+                    if (lane == 0) {
+                        facs[m] = fac;
+                        alist[m] = a;
+                        ++nacc;
+                    }
+                    ++m;
+                }
+            }
+        }
+        if (mine) fl[i0 + lane] = (signed char)fvl;
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) rng[q] = r4[q];
+            *att += (unsigned long long)kbs;
+            *acc += nacc;
+            ch->pcalls[DQMC_PH_PROPOSE] += NS * nacc;   /* green_delay_accept calls */
+            s.iscr[2 * DQMC_MAX_KB] = m;
+            if (neg) ch->sign = -ch->sign;
+        }
+    }
+    __syncthreads();
+    pc.charge(ch, DQMC_PH_PROPOSE);
+    const int m = s.iscr[2 * DQMC_MAX_KB];
+    if constexpr (NS == 2) {
+        if (m > 0)
+            block_flush(n, kb, i0, m, Gd, Zsd, Ysd, 0, true, RrowD, CcolD, facsD, RrowD, s, ch,
+                        pc);
+    }
+    return block_flush(n, kb, i0, m, G, Zs, Ys, mA, flush, Rrow, Ccol, facs, Rrow, s, ch, pc);
+}
+
 /* max|G - Gn| and G <- Gn */
 __device__ double adopt_green(int n, double *G, const double *Gn, Smem &s)
 {
@@ -427,14 +486,15 @@ __device__ double max_diff(int n, const double *A, const double *B, Smem &s)
 /* G(l0) from scratch: L single-slice lmuls then (1+UDT)^{-1} (green.c:262).
  * Uses the chain's scr UDV slot; returns det sign (0 on failure). */
 __device__ __noinline__ int green_scratch(DqmcChainDev *ch, const DqmcModelDev &md, int l0, double *Gout,
-                             double *slot, Smem &s, int *flag)
+                             double *slot, Smem &s, int *flag, int spin = 0)
 {
     const int n = ch->n, L = ch->L;
+    const double *v = spin ? md.expvd : md.expv;
     Udv u = udv_at(slot, n);
     udv_identity(u, n);
     for (int k = 0; k < L; ++k) {
         const int l = (l0 + k) % L;
-        udv_lmul(n, u, nullptr, md.expK, ch->field + (size_t)l * n, md.expv[0], md.expv[1],
+        udv_lmul(n, u, nullptr, md.expK, ch->field + (size_t)l * n, v[0], v[1],
                  chain_scr(ch), s, flag);
         if (*flag) return 0;
     }
@@ -502,7 +562,8 @@ __device__ void ell_stats(int n, const double *ell, double *o, Smem &s)
  * 196-230) of the factor L (and R for a boundary pair) into the chain's
  * record buffer; a no-op unless the engine enabled the records. */
 __device__ __noinline__ void udv_record(DqmcChainDev *ch, int kind, int tau, int boundary, int n,
-                                        const double *ellL, const double *ellR, Smem &s)
+                                        const double *ellL, const double *ellR, Smem &s,
+                                        int spin = 0)
 {
     if (!ch->udvrec) return;
     double a[5], b[5] = {NAN, NAN, 0.0, 0.0, 0.0};
@@ -520,7 +581,7 @@ __device__ __noinline__ void udv_record(DqmcChainDev *ch, int kind, int tau, int
                 r[DQMC_UDV_R_RIGHT + k] = b[k];
             }
             r[DQMC_UDV_R_HAS_RIGHT] = ellR ? 1.0 : 0.0;
-            r[DQMC_UDV_R_HAS_RIGHT + 1] = 0.0;
+            r[DQMC_UDV_R_SPIN] = spin;
             ch->udv_n++;
         } else {
             ch->udv_lost++;
@@ -531,6 +592,22 @@ __device__ __noinline__ void udv_record(DqmcChainDev *ch, int kind, int tau, int
 /* The forward sweep, dqmc_sweep_forward (dqmc.c:609-813) with
  * carry_prefix = 0, use_ph = 1 and the combine rebuild.  Returns false on a
  * numerical failure (flag holds the reason). */
+/* One evolved spin's state: G_up (sigma = +1) or, on the two-spin path,
+ * G_down (sigma = -1) with its own B factors (green_alloc, green.c:54-86). */
+struct Spin {
+    double *G, *S, *left, *comb, *bcache;
+    double v0, v1, vi0, vi1;
+};
+
+__device__ __forceinline__ Spin spin_of(DqmcChainDev *ch, const DqmcModelDev &md, int q)
+{
+    if (q == 0)
+        return Spin{ch->G, ch->S, ch->left, ch->comb, ch->bcache, md.expv[0], md.expv[1],
+                    md.expvinv[0], md.expvinv[1]};
+    return Spin{ch->Gd, ch->Sd, ch->leftd, ch->combd, ch->bcached, md.expvd[0], md.expvd[1],
+                md.expvinvd[0], md.expvinvd[1]};
+}
+
 __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md, int kflags, Smem &s,
                            int *flag, uint64_t *rng, unsigned long long *att,
                            unsigned long long *acc, double *slot_scr)
@@ -538,11 +615,9 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
     const int n = ch->n, L = ch->L, stab = ch->stab, M = ch->M, kb = ch->kb;
     const size_t nn = (size_t)n * n, usz = DQMC_UDV_SIZE(n);
     const Scr w = chain_scr(ch);
-    double *G = ch->G, *Gn = ch->w[3], *tmp = ch->w[4], *tmp2 = ch->w[5];
-    const double v0 = md.expv[0], v1 = md.expv[1];
-    auto Sj = [&](int j) { return udv_at(ch->S + (size_t)j * usz, n); };
+    double *Gn = ch->w[3], *tmp = ch->w[4], *tmp2 = ch->w[5];
+    const int ns = ch->ns;   /* 1: PH path; 2: G_up and G_down (dqmc.c:641-683) */
     auto Pj = [&](int j) { return udv_at(ch->P + (size_t)j * usz, n); };
-    Udv left = udv_at(ch->left, n), comb = udv_at(ch->comb, n);
     const bool alt = ch->alt != 0;
     PhaseClock pc;
     pc.mark();
@@ -550,53 +625,72 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
     /* alternating order with a suffix stack carried from the backward sweep
      * before (dqmc.c:622-629): no stack build */
     if (!(alt && ch->svalid)) {
-        /* Block products B(b_{j+1}, b_j) of the current field.  After the
-         * first sweep they are the ones the previous sweep computed. */
-        if (!ch->bvalid) {
-            for (int j = 1; j < M; ++j) {
-                const int b0 = j * stab, b1 = min((j + 1) * stab, L);
-                bblock(n, b0, b1 - b0, ch->field, md.expK, v0, v1, ch->bcache + j * nn, tmp,
-                       tmp2, s);
+        for (int q = 0; q < ns; ++q) {   /* G_up's stack, then G_down's (dqmc.c:630-646) */
+            const Spin sp = spin_of(ch, md, q);
+            auto Sj = [&](int j) { return udv_at(sp.S + (size_t)j * usz, n); };
+            /* Block products B(b_{j+1}, b_j) of the current field.  After the
+             * first sweep they are the ones the previous sweep computed. */
+            if (!ch->bvalid) {
+                for (int j = 1; j < M; ++j) {
+                    const int b0 = j * stab, b1 = min((j + 1) * stab, L);
+                    bblock(n, b0, b1 - b0, ch->field, md.expK, sp.v0, sp.v1,
+                           sp.bcache + j * nn, tmp, tmp2, s);
+                }
+            }
+            pc.charge(ch, DQMC_PH_BCACHE, 1);
+            /* suffix stack (green_stack_build_suffix, green.c:203-226) */
+            udv_identity(Sj(M), n);
+            for (int j = M - 1; j >= 1; --j) {
+                udv_copy(Sj(j), Sj(j + 1), n);
+                udv_record(ch, DQMC_UDV_STACK_SUFFIX_PRE_RMUL, min(j * stab, L), j, n, Sj(j).ell,
+                           nullptr, s, q);
+                if (threadIdx.x == 0) ch->pcalls[DQMC_PH_STACK]++;   /* udv_rmul calls */
+                udv_rmul(n, Sj(j), sp.bcache + j * nn, w, s, flag);
+                if (*flag) return false;
             }
         }
-        pc.charge(ch, DQMC_PH_BCACHE, 1);
-        /* suffix stack (green_stack_build_suffix, green.c:203-226) */
-        udv_identity(Sj(M), n);
-        for (int j = M - 1; j >= 1; --j) {
-            udv_copy(Sj(j), Sj(j + 1), n);
-            udv_record(ch, DQMC_UDV_STACK_SUFFIX_PRE_RMUL, min(j * stab, L), j, n, Sj(j).ell,
-                       nullptr, s);
-            if (threadIdx.x == 0) ch->pcalls[DQMC_PH_STACK]++;   /* udv_rmul calls */
-            udv_rmul(n, Sj(j), ch->bcache + j * nn, w, s, flag);
-            if (*flag) return false;
-        }
     }
-    udv_identity(left, n);
-    if (alt) udv_copy(Pj(0), left, n);   /* prefix stack (dqmc.c:648-650) */
+    for (int q = 0; q < ns; ++q) udv_identity(udv_at(spin_of(ch, md, q).left, n), n);
+    if (alt) udv_copy(Pj(0), udv_at(ch->left, n), n);   /* prefix stack (dqmc.c:648-650) */
     pc.charge(ch, DQMC_PH_STACK);
     int tau_left = 0;
     for (int l = 0; l < L; ++l) {
         signed char *fl = ch->field + (size_t)l * n;
-        for (int i0 = 0, mA = 0; i0 < n; i0 += kb)
-            mA = site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs,
-                            ch->Ys, mA, !ch->pair || mA > 0 || i0 + kb >= n, s, ch, pc);
+        if (ns == 2) {
+            for (int i0 = 0; i0 < n; i0 += kb)
+                site_block<2>(n, kb, min(kb, n - i0), i0, ch->G, fl, md, rng, att, acc, ch->Zs,
+                              ch->Ys, 0, true, s, ch, pc, ch->Gd, ch->Zsd, ch->Ysd);
+        } else {
+            for (int i0 = 0, mA = 0; i0 < n; i0 += kb)
+                mA = site_block<1>(n, kb, min(kb, n - i0), i0, ch->G, fl, md, rng, att, acc,
+                                   ch->Zs, ch->Ys, mA, !ch->pair || mA > 0 || i0 + kb >= n, s,
+                                   ch, pc);
+        }
+        for (int q = 0; q < ns; ++q) {
+            const Spin sp = spin_of(ch, md, q);
 #if DQMC_MINB == 1
-        if (kflags & KF_MIXED)
-            wrap_green_mixed(n, G, tmp, md, fl, v0, v1, md.expvinv[0], md.expvinv[1], ch->mix,
-                             ch->mix_ex, s);
-        else
+            if (kflags & KF_MIXED)
+                wrap_green_mixed(n, sp.G, tmp, md, fl, sp.v0, sp.v1, sp.vi0, sp.vi1, ch->mix,
+                                 ch->mix_ex, s);
+            else
 #endif
-            wrap_green(n, G, tmp, md.expK, md.expKinv, fl, v0, v1, md.expvinv[0],
-                       md.expvinv[1], s);
-        pc.charge(ch, DQMC_PH_WRAP, 1);
+                wrap_green(n, sp.G, tmp, md.expK, md.expKinv, fl, sp.v0, sp.v1, sp.vi0, sp.vi1,
+                           s);
+            pc.charge(ch, DQMC_PH_WRAP, 1);
+        }
         const bool boundary = ((l + 1) % stab == 0) && (l + 1 < L);
         const bool last = (l + 1 == L);
         if (!boundary && !last) continue;
         const int tau = boundary ? l + 1 : 0;
         if (kflags & KF_SDRIFT) {
-            const int ds = green_scratch(ch, md, tau, Gn, slot_scr, s, flag);
-            if (*flag || ds == 0) return false;
-            const double d = max_diff(n, G, Gn, s);
+            /* dqmc_record_stab_drift (dqmc.c:64-98): both spins, the larger */
+            double d = 0.0;
+            for (int q = 0; q < ns; ++q) {
+                const int ds = green_scratch(ch, md, tau, Gn, slot_scr, s, flag, q);
+                if (*flag || ds == 0) return false;
+                d = fmax(d, max_diff(n, spin_of(ch, md, q).G, Gn, s));
+                pc.charge(ch, DQMC_PH_SDRIFT, 1);
+            }
             if (threadIdx.x == 0) {
                 ch->sdrift_count++;
                 ch->sdrift_sum += d;
@@ -606,54 +700,73 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
                     ch->sdrift_max_sweep = ch->sweeps;
                 }
             }
-            pc.charge(ch, DQMC_PH_SDRIFT, 1);
         }
         const int te = boundary ? l + 1 : L;
         const int jblk = (boundary ? (l + 1) / stab : M) - 1;
-        if (te > tau_left) {
-            bblock(n, tau_left, te - tau_left, ch->field, md.expK, v0, v1,
-                   ch->bcache + jblk * nn, tmp, tmp2, s);
-            pc.charge(ch, DQMC_PH_BBLOCK, 1);
-            udv_lmul(n, left, ch->bcache + jblk * nn, nullptr, nullptr, 0.0, 0.0, w, s, flag);
-            if (*flag) return false;
-            pc.charge(ch, DQMC_PH_LMUL, 1);
+        for (int q = 0; q < ns; ++q) {
+            const Spin sp = spin_of(ch, md, q);
+            if (te > tau_left) {
+                bblock(n, tau_left, te - tau_left, ch->field, md.expK, sp.v0, sp.v1,
+                       sp.bcache + jblk * nn, tmp, tmp2, s);
+                pc.charge(ch, DQMC_PH_BBLOCK, 1);
+                udv_lmul(n, udv_at(sp.left, n), sp.bcache + jblk * nn, nullptr, nullptr, 0.0, 0.0,
+                         w, s, flag);
+                if (*flag) return false;
+                pc.charge(ch, DQMC_PH_LMUL, 1);
+            }
         }
         tau_left = te;
-        if (alt) udv_copy(Pj(boundary ? (l + 1) / stab : M), left, n);   /* dqmc.c:704-706,767 */
-        if (boundary)   /* dqmc.c:707-715, 772-779 */
-            udv_record(ch, DQMC_UDV_FORWARD, l + 1, (l + 1) / stab, n, left.ell,
-                       Sj((l + 1) / stab).ell, s);
-        else
-            udv_record(ch, DQMC_UDV_LEFT_FORWARD, L, M, n, left.ell, nullptr, s);
-        int ds;
-        if (boundary && ch->rebuild) {
-            ds = udv_green2(n, left, Sj((l + 1) / stab), Gn, tmp2, w, s, flag);
-        } else if (boundary) {
-            udv_combine(n, left, Sj((l + 1) / stab), comb, w, s, flag);
-            if (*flag) return false;
-            pc.charge(ch, DQMC_PH_COMBINE, 1);
-            ds = udv_green(n, comb, Gn, w, s, flag);
-        } else {
-            ds = udv_green(n, left, Gn, w, s, flag);
+        if (alt)   /* dqmc.c:704-706,767 */
+            udv_copy(Pj(boundary ? (l + 1) / stab : M), udv_at(ch->left, n), n);
+        for (int q = 0; q < ns; ++q) {   /* dqmc.c:707-724, 772-789 */
+            const Spin sp = spin_of(ch, md, q);
+            if (boundary)
+                udv_record(ch, DQMC_UDV_FORWARD, l + 1, (l + 1) / stab, n, udv_at(sp.left, n).ell,
+                           udv_at(sp.S + (size_t)((l + 1) / stab) * usz, n).ell, s, q);
+            else
+                udv_record(ch, DQMC_UDV_LEFT_FORWARD, L, M, n, udv_at(sp.left, n).ell, nullptr, s,
+                           q);
         }
-        pc.charge(ch, DQMC_PH_GREEN, 1);
-        if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
-        __syncthreads();
-        if (*flag) return false;
-        const double d = adopt_green(n, G, Gn, s);
-        /* a wrapped G that is not finite means the chain's state was lost
-         * since the last rebuild: stop the chain (sticky status) */
-        if (!(d == d) || isinf(d)) {
-            raise_flag(flag, DQMC_ST_NONFINITE);
-            return false;
+        double d = 0.0;
+        int sgn = 1;
+        for (int q = 0; q < ns; ++q) {   /* green_from_stack / _left_udv per spin */
+            const Spin sp = spin_of(ch, md, q);
+            Udv left = udv_at(sp.left, n), comb = udv_at(sp.comb, n);
+            Udv Sb = udv_at(sp.S + (size_t)((l + 1) / stab) * usz, n);
+            int ds;
+            if (boundary && ch->rebuild) {
+                ds = udv_green2(n, left, Sb, Gn, tmp2, w, s, flag);
+            } else if (boundary) {
+                udv_combine(n, left, Sb, comb, w, s, flag);
+                if (*flag) return false;
+                pc.charge(ch, DQMC_PH_COMBINE, 1);
+                ds = udv_green(n, comb, Gn, w, s, flag);
+            } else {
+                ds = udv_green(n, left, Gn, w, s, flag);
+            }
+            pc.charge(ch, DQMC_PH_GREEN, 1);
+            if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
+            __syncthreads();
+            if (*flag) return false;
+            sgn *= ds;
+            const double dq = adopt_green(n, sp.G, Gn, s);
+            /* a wrapped G that is not finite means the chain's state was lost
+             * since the last rebuild: stop the chain (sticky status) */
+            if (!(dq == dq) || isinf(dq)) {
+                raise_flag(flag, DQMC_ST_NONFINITE);
+                return false;
+            }
+            d = fmax(d, dq);
+            pc.charge(ch, DQMC_PH_ADOPT, 1);
         }
         if (threadIdx.x == 0) {
             ch->drift_count++;
             ch->drift_sum += d;
             if (d > ch->drift_max || ch->drift_count == 1) ch->drift_max = d;
-            ch->sign = 1.0;
+            /* the running sign reset to the stabilized exact value
+             * (dqmc.c:740-745): 1 on the PH path, det_up * det_down else */
+            ch->sign = ns == 2 ? (double)sgn : 1.0;
         }
-        pc.charge(ch, DQMC_PH_ADOPT, 1);
     }
     return true;
 }
@@ -763,8 +876,8 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     for (int l = L - 1; l >= 0; --l) {
         signed char *fl = ch->field + (size_t)l * n;
         for (int i0 = 0, mA = 0; i0 < n; i0 += kb)
-            mA = site_block(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs,
-                            ch->Ys, mA, !ch->pair || mA > 0 || i0 + kb >= n, s, ch, pc);
+            mA = site_block<1>(n, kb, min(kb, n - i0), i0, G, fl, md, rng, att, acc, ch->Zs,
+                               ch->Ys, mA, !ch->pair || mA > 0 || i0 + kb >= n, s, ch, pc);
         if (l == 0) break;
         if (l % stab == 0 && !rebuild(l, left, true, l / stab)) return false;
         back_wrap(l - 1);
@@ -833,11 +946,14 @@ __global__ void __launch_bounds__(NT, DQMC_MINB) k_init(DqmcChainDev *chains, co
     if (threadIdx.x == 0) flag = 0;
     __syncthreads();
     Smem s = carve(smraw, ch->n, ch->kb);
-    const int ds = green_scratch(ch, md, 0, ch->G, ch->scr, s, &flag);
+    int ds = green_scratch(ch, md, 0, ch->G, ch->scr, s, &flag);
+    /* the two-spin path starts with the sign det_up * det_down
+     * (dqmc.c:467-481) */
+    if (ch->ns == 2 && !flag) ds *= green_scratch(ch, md, 0, ch->Gd, ch->scr, s, &flag, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         ch->status = flag ? flag : (ds == 0 ? DQMC_ST_DETSIGN : 0);
-        ch->sign = ch->status ? 0.0 : 1.0;
+        ch->sign = ch->status ? 0.0 : (ch->ns == 2 ? (double)ds : 1.0);
         ch->bvalid = 0;
         ch->dir = 0;
         ch->pvalid = 0;
@@ -934,20 +1050,25 @@ __global__ void __launch_bounds__(NT)
     const double *G = ch->G;
     const double *t = md.thop;
     const int *p = md.bipart;
+    /* G_down: the PH map of G_up (dqmc_map_ph_down, dqmc.c:9-17), or the
+     * evolved G_down of the two-spin path */
+    const double *Gd = ch->Gd;
+    const bool two = ch->ns == 2;
     double ek = 0.0, ei = 0.0, nt = 0.0, bad = 0.0;
     for (int e = threadIdx.x; e < n * n; e += NT) {
         const int i = e % n, j = e / n;
         const double dij = (i == j) ? 1.0 : 0.0;
         const double gu_ji = G[j + (size_t)i * n];
-        const double gd_ji = dij - (double)(p[j] * p[i]) * G[i + (size_t)j * n];
+        const double gd_ji = two ? Gd[j + (size_t)i * n]
+                                 : dij - (double)(p[j] * p[i]) * G[i + (size_t)j * n];
         const double tij = t[i + (size_t)j * n];
         ek += tij * (dij - gu_ji);
         ek += tij * (dij - gd_ji);
-        bad += isfinite(gu_ji) ? 0.0 : 1.0;
+        bad += isfinite(gu_ji) && isfinite(gd_ji) ? 0.0 : 1.0;
     }
     for (int i = threadIdx.x; i < n; i += NT) {
         const double gu = G[i + (size_t)i * n];
-        const double gd = 1.0 - (double)(p[i] * p[i]) * gu;
+        const double gd = two ? Gd[i + (size_t)i * n] : 1.0 - (double)(p[i] * p[i]) * gu;
         const double nu = 1.0 - gu, nd = 1.0 - gd;
         ei += nu * nd;
         nt += nu + nd;
@@ -975,10 +1096,10 @@ __global__ void __launch_bounds__(NT)
                 const double pij = (double)(p[i] * p[j]);
                 const double gu_ii = G[i + (size_t)i * n], gu_jj = G[j + (size_t)j * n];
                 const double gu_ij = G[i + (size_t)j * n], gu_ji = G[j + (size_t)i * n];
-                const double gd_ii = 1.0 - (double)(p[i] * p[i]) * gu_ii;
-                const double gd_jj = 1.0 - (double)(p[j] * p[j]) * gu_jj;
-                const double gd_ij = delta - pij * gu_ji;
-                const double gd_ji = delta - pij * gu_ij;
+                const double gd_ii = two ? Gd[i + (size_t)i * n] : 1.0 - (double)(p[i] * p[i]) * gu_ii;
+                const double gd_jj = two ? Gd[j + (size_t)j * n] : 1.0 - (double)(p[j] * p[j]) * gu_jj;
+                const double gd_ij = two ? Gd[i + (size_t)j * n] : delta - pij * gu_ji;
+                const double gd_ji = two ? Gd[j + (size_t)i * n] : delta - pij * gu_ij;
                 const double spin_i = gd_ii - gu_ii, spin_j = gd_jj - gu_jj;
                 sz += 0.25 * (spin_i * spin_j + (delta - gu_ji) * gu_ij + (delta - gd_ji) * gd_ij);
                 sp += 0.5 * ((delta - gu_ji) * gd_ij + (delta - gd_ji) * gu_ij);

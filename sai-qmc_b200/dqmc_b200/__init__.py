@@ -78,6 +78,9 @@ def lib():
     L.dqmc_engine_destroy.argtypes = [C.c_void_p]
     L.dqmc_model_add.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, _ip,
                                  C.c_double, C.c_double]
+    L.dqmc_model_add_mu.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, C.c_void_p,
+                                    C.c_double, C.c_double, C.c_int, C.c_double, C.c_int]
+    L.dqmc_read_green_down.argtypes = [C.c_void_p, C.c_int, _dp]
     L.dqmc_model_set_spin.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.dqmc_chain_add.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
@@ -220,12 +223,18 @@ class Engine:
         self.nbin = 0
 
     def add_model(self, thop, bipart, U, dtau, Lx=0, Ly=0, szz="none",
-                  sperp="none"):
+                  sperp="none", mu=None, two_spin=False):
+        """mu=None: half filling (mu = U/2).  bipart=None (non-bipartite
+        lattice), a mu off half filling or two_spin=True: the two-spin path
+        (G_up and G_down evolved separately)."""
         thop = np.asarray(thop, dtype=np.float64)
         n = thop.shape[0]
-        mid = lib().dqmc_model_add(self.h, n, Lx, Ly, _cm(thop),
-                                   np.ascontiguousarray(bipart, dtype=np.int32),
-                                   U, dtau)
+        bp = None if bipart is None else np.ascontiguousarray(bipart, dtype=np.int32)
+        self._bp = bp
+        mid = lib().dqmc_model_add_mu(self.h, n, Lx, Ly, _cm(thop),
+                                      None if bp is None else bp.ctypes.data_as(C.c_void_p),
+                                      U, dtau, 1 if mu is None else 0,
+                                      0.0 if mu is None else float(mu), int(two_spin))
         if mid < 0:
             raise DqmcError(lib().dqmc_last_error().decode())
         zx, zy = q_list(Lx, Ly, szz) if szz != "none" else ([], [])
@@ -268,6 +277,12 @@ class Engine:
         n = self.chains[c]["n"]
         g = np.zeros(n * n)
         _check(lib().dqmc_read_green(self.h, c, g), "read_green")
+        return _from_cm(g, n)
+
+    def green_down(self, c):
+        n = self.chains[c]["n"]
+        g = np.zeros(n * n)
+        _check(lib().dqmc_read_green_down(self.h, c, g), "read_green_down")
         return _from_cm(g, n)
 
     def field(self, c):

@@ -299,6 +299,7 @@ static int write_udv_records(const DqmcParams *p, dqmc_engine *e, int chain, int
             const unsigned long long sw = (unsigned long long)x[DQMC_UDV_R_SWEEP];
             const double *lf = x + DQMC_UDV_R_LEFT, *rt = x + DQMC_UDV_R_RIGHT;
             const int pair = x[DQMC_UDV_R_HAS_RIGHT] != 0.0;
+            const char *spin = x[DQMC_UDV_R_SPIN] != 0.0 ? "d" : "u";
             if (fs) {
                 const double lsp = lf[2] > 0 ? lf[1] - lf[0] : NAN;
                 const double rsp = rt[2] > 0 ? rt[1] - rt[0] : NAN;
@@ -307,7 +308,7 @@ static int write_udv_records(const DqmcParams *p, dqmc_engine *e, int chain, int
                 fprintf(fs,
                         "%d %d %d %llu %.17g %.17g %d %llu %d %d %s %s %.17g %.17g %.17g %d %d "
                         "%d %.17g %.17g %.17g %d %d %d %.17g\n",
-                        b, Ltr, r, seed, p->U, p->dtau, p->stab_interval, sw, tau, bnd, "u",
+                        b, Ltr, r, seed, p->U, p->dtau, p->stab_interval, sw, tau, bnd, spin,
                         udv_direction(kind), lf[0], lf[1], lsp, (int)lf[2], (int)lf[3],
                         (int)lf[4], rt[0], rt[1], rsp, (int)rt[2], (int)rt[3], (int)rt[4],
                         cross);
@@ -344,7 +345,7 @@ static int write_udv_records(const DqmcParams *p, dqmc_engine *e, int chain, int
                 fprintf(fc,
                         "%d %d %d %llu %llu %d %d %s %s %.17g %.17g %.17g %.17g %.17g %.17g "
                         "%.17g %d %s\n",
-                        b, Ltr, r, seed, sw, tau, bnd, "u", udv_direction(kind), smin, smax, rad,
+                        b, Ltr, r, seed, sw, tau, bnd, spin, udv_direction(kind), smin, smax, rad,
                         off, emin, emax, margin, warning, status);
                 if (fail) {
                     fprintf(stderr, "ERROR: centered UDV diagnostic failed (beta_index=%d "

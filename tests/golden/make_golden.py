@@ -7,7 +7,8 @@ oracle/ref_shim.c and writes small .npz files next to this script.  The
 reference's own UDV fixtures (tests/fixtures/udv_phase6a_*.txt, read here as
 data) are re-packed into udv_fixture.npz.  ``--only-alternating`` writes
 just the sweep_order=alternating fixtures (*_alt.npz), ``--only-rebuild``
-the green_rebuild=two_sided/centered ones.  The GPU box never needs the
+the green_rebuild=two_sided/centered ones, ``--only-two-spin`` the
+two-spin (use_ph = 0) ones.  The GPU box never needs the
 reference: tests read only the .npz files.
 """
 from __future__ import annotations
@@ -55,6 +56,14 @@ REBUILD_CASES = [
     ("sq8_b4_2s", LAT_SQUARE, 8, 8, 4.0, 0.1, 40, 10, 7, 3, False, 1),
     ("chain4_ctr", LAT_CHAIN, 4, 1, 4.0, 0.1, 20, 8, 1, 3, False, 2),
     ("sq6_b2_2s_alt", LAT_SQUARE, 6, 6, 6.0, 0.1, 20, 8, 3, 4, True, 1),
+]
+# the two-spin path (use_ph = 0, dqmc.c:641-813): forced at the PH point,
+# a non-bipartite chain at half filling, a doped square lattice
+# (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, half, mu, force)
+TWO_SPIN_CASES = [
+    ("sq4_2spin", LAT_SQUARE, 4, 4, 4.0, 0.1, 20, 5, 5, 3, 1, 0.0, 1),
+    ("chain3_2spin", LAT_CHAIN, 3, 1, 4.0, 0.1, 10, 4, 19, 4, 1, 0.0, 0),
+    ("sq4_mu", LAT_SQUARE, 4, 4, 4.0, 0.1, 20, 5, 7, 3, 0, 0.7, 0),
 ]
 HEADLINE_ALT = dict(Lx=16, U=4.0, dtau=0.1, L=80, stab=8, base_seed=11, chains=2, sweeps=4)
 
@@ -185,6 +194,32 @@ def rebuild_modes(R):
                         det_sign=int(rec["det_sign"][0]))
 
 
+def two_spin(R):
+    for (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, half, mu, force) in TWO_SPIN_CASES:
+        ch = R.chain_mu(kind, Lx, Ly, U, dtau, L, stab, seed, half=bool(half), mu=mu,
+                        two_spin=bool(force))
+        st0 = ch.state()
+        fields, Gu, Gd, cnt, sign, meas = [], [], [], [], [], []
+        for _ in range(sweeps):
+            ch.sweep(1)
+            st = ch.state()
+            fields.append(st["field"])
+            Gu.append(st["Gu"])
+            Gd.append(st["Gd"])
+            sign.append(st["sign"])
+            cnt.append([st["attempts"], st["accepted"], st["sweeps"], st["status"]])
+            m, _, _ = R.measure(ch, None)
+            meas.append(m)
+        np.savez_compressed(
+            os.path.join(HERE, f"{name}.npz"),
+            params=np.array([kind, Lx, Ly, L, stab, seed, sweeps, half, force], dtype=np.int64),
+            U=U, dtau=dtau, mu=mu, field0=st0["field"], Gu0=st0["Gu"], Gd0=st0["Gd"],
+            sign0=st0["sign"], fields=np.array(fields), Gu=np.array(Gu), Gd=np.array(Gd),
+            sign=np.array(sign), counters=np.array(cnt, dtype=np.int64), meas=np.array(meas),
+            rng_end=st["rng"])
+        ch.free()
+
+
 def headline_alt_fields():
     """Fields of the alternating headline chains, written as .npy to stdout."""
     R = Reference()
@@ -214,6 +249,10 @@ def main():
     if "--only-alternating" in sys.argv:
         alternating(R)
         print("wrote alternating fixtures")
+        return
+    if "--only-two-spin" in sys.argv:
+        two_spin(R)
+        print("wrote two-spin fixtures")
         return
     if "--only-rebuild" in sys.argv:
         rebuild_modes(R)
