@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstddef>
 #include <cstdarg>
 #include <cstdio>
@@ -69,45 +70,129 @@ double host_rng_next(uint64_t *s)
 
 /* Symmetric eigendecomposition by cyclic Jacobi rotations; A is overwritten
  * by its eigenvalues on the diagonal, V receives the eigenvectors. */
-void jacobi_eig(int n, std::vector<double> &a, std::vector<double> &V)
+/* Symmetric eigendecomposition A = Z diag(w) Z^T (column-major n x n), as
+ * the reference's dsyev call in la_expm_sym (src/linalg.c:319-346) provides
+ * it: Householder reduction to tridiagonal form with the reflectors
+ * accumulated, then implicit symmetric QR steps with Wilkinson shifts on the
+ * tridiagonal (Golub & Van Loan, Matrix Computations, Algorithms 5.1.1,
+ * 8.3.1 and 8.3.2-8.3.3).  O(n^3) with a small constant: about 0.1 s at
+ * n = 256 where cyclic Jacobi took seconds. */
+void sym_eig(int n, const double *A, std::vector<double> &w, std::vector<double> &Z)
 {
-    V.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) V[i + (size_t)i * n] = 1.0;
-    for (int sweep = 0; sweep < 60; ++sweep) {
-        double off = 0.0, diag = 0.0;
-        for (int j = 0; j < n; ++j) {
-            diag += a[j + (size_t)j * n] * a[j + (size_t)j * n];
-            for (int i = 0; i < j; ++i) off += a[i + (size_t)j * n] * a[i + (size_t)j * n];
+    std::vector<double> a(A, A + (size_t)n * n);
+    auto at = [&](int i, int j) -> double & { return a[i + (size_t)j * n]; };
+    std::vector<double> vs((size_t)n * n, 0.0), betas(n, 0.0), pv(n), wv(n);
+    /* tridiagonalization: H_k = I - beta v v^T on rows / columns k+1 .. n-1 */
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        double *v = &vs[(size_t)k * n];
+        double sigma = 0.0;
+        for (int i = 1; i < m; ++i) sigma += at(k + 1 + i, k) * at(k + 1 + i, k);
+        if (sigma == 0.0) continue;          /* column already tridiagonal */
+        const double x0 = at(k + 1, k);
+        const double mu = std::sqrt(x0 * x0 + sigma);
+        const double v0 = x0 <= 0.0 ? x0 - mu : -sigma / (x0 + mu);
+        const double beta = 2.0 * v0 * v0 / (sigma + v0 * v0);
+        v[0] = 1.0;
+        for (int i = 1; i < m; ++i) v[i] = at(k + 1 + i, k) / v0;
+        betas[k] = beta;
+        /* p = beta A22 v (column sweeps), w = p - (beta p^T v / 2) v */
+        for (int i = 0; i < m; ++i) pv[i] = 0.0;
+        for (int j = 0; j < m; ++j) {
+            const double vj = beta * v[j];
+            const double *col = &at(k + 1, k + 1 + j);
+            for (int i = 0; i < m; ++i) pv[i] += col[i] * vj;
         }
-        if (off <= 1e-34 * (diag + 1e-300)) break;
-        for (int p = 0; p < n - 1; ++p)
-            for (int q = p + 1; q < n; ++q) {
-                const double apq = a[p + (size_t)q * n];
-                if (apq == 0.0) continue;
-                const double app = a[p + (size_t)p * n], aqq = a[q + (size_t)q * n];
-                const double theta = (aqq - app) / (2.0 * apq);
-                const double tt = (theta >= 0 ? 1.0 : -1.0) /
-                                  (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                const double c = 1.0 / std::sqrt(tt * tt + 1.0), s = tt * c;
-                for (int k = 0; k < n; ++k) {
-                    double &akp = a[k + (size_t)p * n], &akq = a[k + (size_t)q * n];
-                    const double x = akp, y = akq;
-                    akp = c * x - s * y;
-                    akq = s * x + c * y;
-                }
-                for (int k = 0; k < n; ++k) {
-                    double &apk = a[p + (size_t)k * n], &aqk = a[q + (size_t)k * n];
-                    const double x = apk, y = aqk;
-                    apk = c * x - s * y;
-                    aqk = s * x + c * y;
-                }
-                for (int k = 0; k < n; ++k) {
-                    double &vkp = V[k + (size_t)p * n], &vkq = V[k + (size_t)q * n];
-                    const double x = vkp, y = vkq;
-                    vkp = c * x - s * y;
-                    vkq = s * x + c * y;
-                }
+        double ptv = 0.0;
+        for (int i = 0; i < m; ++i) ptv += pv[i] * v[i];
+        const double half = 0.5 * beta * ptv;
+        for (int i = 0; i < m; ++i) wv[i] = pv[i] - half * v[i];
+        /* A22 -= v w^T + w v^T */
+        for (int j = 0; j < m; ++j) {
+            double *col = &at(k + 1, k + 1 + j);
+            const double wj = wv[j], vj = v[j];
+            for (int i = 0; i < m; ++i) col[i] -= v[i] * wj + wv[i] * vj;
+        }
+        at(k + 1, k) = mu;
+        at(k, k + 1) = mu;
+        for (int i = 1; i < m; ++i) {
+            at(k + 1 + i, k) = 0.0;
+            at(k, k + 1 + i) = 0.0;
+        }
+    }
+    /* Q = H_0 ... H_{n-3} by backward accumulation (Golub & Van Loan 5.1.6) */
+    Z.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) Z[i + (size_t)i * n] = 1.0;
+    for (int k = n - 3; k >= 0; --k) {
+        if (betas[k] == 0.0) continue;
+        const int m = n - k - 1;
+        const double *v = &vs[(size_t)k * n];
+        for (int j = k + 1; j < n; ++j) {
+            double *col = &Z[(k + 1) + (size_t)j * n];
+            double sdot = 0.0;
+            for (int i = 0; i < m; ++i) sdot += v[i] * col[i];
+            sdot *= betas[k];
+            for (int i = 0; i < m; ++i) col[i] -= sdot * v[i];
+        }
+    }
+    std::vector<double> d(n), e(n > 1 ? n - 1 : 1, 0.0);
+    for (int i = 0; i < n; ++i) d[i] = at(i, i);
+    for (int i = 0; i + 1 < n; ++i) e[i] = at(i + 1, i);
+    /* implicit symmetric QR with Wilkinson shifts; Z <- Z R^T per rotation */
+    const double eps = std::numeric_limits<double>::epsilon();
+    int q = n - 1, guard = 0;
+    while (q > 0 && guard < 64 * n) {
+        for (int i = 0; i < q; ++i)
+            if (std::fabs(e[i]) <= eps * (std::fabs(d[i]) + std::fabs(d[i + 1]))) e[i] = 0.0;
+        if (e[q - 1] == 0.0) {
+            --q;
+            continue;
+        }
+        int p = q - 1;
+        while (p > 0 && e[p - 1] != 0.0) --p;
+        ++guard;
+        const double dd = 0.5 * (d[q - 1] - d[q]), ee = e[q - 1];
+        const double mu = d[q] - ee * ee / (dd + std::copysign(std::hypot(dd, ee), dd));
+        double x = d[p] - mu, z = e[p], bulge = 0.0;
+        for (int k = p; k < q; ++k) {
+            const double r = std::hypot(x, z);
+            const double c = r == 0.0 ? 1.0 : x / r, sn = r == 0.0 ? 0.0 : z / r;
+            if (k > p) e[k - 1] = r;
+            const double ak = d[k], bk = e[k], ck = d[k + 1];
+            d[k] = c * c * ak + 2.0 * c * sn * bk + sn * sn * ck;
+            e[k] = c * sn * (ck - ak) + (c * c - sn * sn) * bk;
+            d[k + 1] = sn * sn * ak - 2.0 * c * sn * bk + c * c * ck;
+            if (k + 1 < q) {
+                bulge = sn * e[k + 1];
+                e[k + 1] *= c;
             }
+            double *zk = &Z[(size_t)k * n], *zk1 = &Z[(size_t)(k + 1) * n];
+            for (int i = 0; i < n; ++i) {
+                const double u = zk[i], t = zk1[i];
+                zk[i] = c * u + sn * t;
+                zk1[i] = -sn * u + c * t;
+            }
+            x = e[k];
+            z = bulge;
+        }
+    }
+    w = d;
+}
+
+/* out_s = Z diag(exp(s_t w)) Z^T for the scales s_0, s_1 of one
+ * decomposition (expK and expK^-1 of a model share it). */
+void expm_from_eig(int n, const std::vector<double> &w, const std::vector<double> &Z,
+                   double scale, double *out)
+{
+    for (size_t i = 0; i < (size_t)n * n; ++i) out[i] = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const double f = std::exp(scale * w[k]);
+        const double *zk = &Z[(size_t)k * n];
+        for (int j = 0; j < n; ++j) {
+            const double fj = f * zk[j];
+            double *col = out + (size_t)j * n;
+            for (int i = 0; i < n; ++i) col[i] += zk[i] * fj;
+        }
     }
 }
 
@@ -199,16 +284,9 @@ void dqmc_desc_default(dqmc_engine_desc *d)
 int dqmc_expm_sym(int n, const double *A, double scale, double *out)
 {
     if (n <= 0 || !A || !out) return set_err("dqmc_expm_sym: bad arguments");
-    std::vector<double> a(A, A + (size_t)n * n), V;
-    jacobi_eig(n, a, V);
-    std::vector<double> f(n);
-    for (int k = 0; k < n; ++k) f[k] = std::exp(scale * a[k + (size_t)k * n]);
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i < n; ++i) {
-            double s = 0.0;
-            for (int k = 0; k < n; ++k) s += V[i + (size_t)k * n] * f[k] * V[j + (size_t)k * n];
-            out[i + (size_t)j * n] = s;
-        }
+    std::vector<double> w, Z;
+    sym_eig(n, A, w, Z);
+    expm_from_eig(n, w, Z, scale, out);
     return 0;
 }
 
@@ -308,8 +386,10 @@ int dqmc_model_add_mu(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
     for (int i = 0; i < n; ++i) K[i + (size_t)i * n] -= m.mu;
     m.expK.resize((size_t)n * n);
     m.expKinv.resize((size_t)n * n);
-    dqmc_expm_sym(n, K.data(), -dtau, m.expK.data());
-    dqmc_expm_sym(n, K.data(), dtau, m.expKinv.data());
+    std::vector<double> w, Z;   /* one decomposition for expK and expK^-1 */
+    sym_eig(n, K.data(), w, Z);
+    expm_from_eig(n, w, Z, -dtau, m.expK.data());
+    expm_from_eig(n, w, Z, dtau, m.expKinv.data());
     e->models.push_back(std::move(m));
     return (int)e->models.size() - 1;
 }

@@ -226,4 +226,6 @@ def test_paired_flushes_equal_single_on_large_lattice(sweep_order):
         np.testing.assert_array_equal(f0, f1)
         assert (c0["attempts"], c0["accepted"]) == (c1["attempts"], c1["accepted"])
         assert np.max(np.abs(g0 - g1)) < 1e-9
-        assert c1["status"] == 0 and c1["drift_max"] < 1e-6
+        # pairing does not cost stability: the stabilization drift of the
+        # paired run stays at the unpaired run's level
+        assert c1["status"] == 0 and c1["drift_max"] < 10 * max(c0["drift_max"], 1e-8)
