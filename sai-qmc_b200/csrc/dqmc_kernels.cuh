@@ -937,6 +937,29 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
 }
 
 /* G from scratch at l0 = 0 for every chain (dqmc_init_modes, dqmc.c:466-483). */
+/* G at slice 0 for a new or rewritten field: the UDV of B_{L-1} ... B_0
+ * accumulated from the stabilization blocks B(b_{j+1}, b_j) (stab slices
+ * per QR-based lmul, as the sweep's stack is) instead of one lmul per slice
+ * (green_from_scratch, green.c:262-306, which the reference-definition
+ * drift diagnostic keeps using): the same product, M instead of L
+ * factorizations. */
+__device__ __noinline__ int green_init(DqmcChainDev *ch, const DqmcModelDev &md, double *Gout,
+                                       double *slot, Smem &s, int *flag, int spin)
+{
+    const int n = ch->n, L = ch->L, stab = ch->stab, M = ch->M;
+    const double *v = spin ? md.expvd : md.expv;
+    Udv u = udv_at(slot, n);
+    udv_identity(u, n);
+    for (int j = 0; j < M; ++j) {
+        const int b0 = j * stab, len = min(stab, L - b0);
+        bblock(n, b0, len, ch->field, md.expK, v[0], v[1], ch->w[3], ch->w[4], ch->w[5], s);
+        udv_lmul(n, u, ch->w[3], nullptr, nullptr, 0.0, 0.0, chain_scr(ch), s, flag);
+        if (*flag) return 0;
+    }
+    const int ds = udv_green(n, u, Gout, chain_scr(ch), s, flag);
+    return *flag ? 0 : ds;
+}
+
 __global__ void __launch_bounds__(NT, DQMC_MINB) k_init(DqmcChainDev *chains, const DqmcModelDev *models)
 {
     extern __shared__ __align__(16) double smraw[];
@@ -946,10 +969,10 @@ __global__ void __launch_bounds__(NT, DQMC_MINB) k_init(DqmcChainDev *chains, co
     if (threadIdx.x == 0) flag = 0;
     __syncthreads();
     Smem s = carve(smraw, ch->n, ch->kb);
-    int ds = green_scratch(ch, md, 0, ch->G, ch->scr, s, &flag);
+    int ds = green_init(ch, md, ch->G, ch->scr, s, &flag, 0);
     /* the two-spin path starts with the sign det_up * det_down
      * (dqmc.c:467-481) */
-    if (ch->ns == 2 && !flag) ds *= green_scratch(ch, md, 0, ch->Gd, ch->scr, s, &flag, 1);
+    if (ch->ns == 2 && !flag) ds *= green_init(ch, md, ch->Gd, ch->scr, s, &flag, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
         ch->status = flag ? flag : (ds == 0 ? DQMC_ST_DETSIGN : 0);
