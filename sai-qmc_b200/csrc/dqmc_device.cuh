@@ -489,7 +489,7 @@ __host__ __device__ inline size_t smem_doubles(int n, int kb)
     const int cb = qr_cb(n);
     const size_t gu = smem_gemm_union(n, cb);
     size_t q = cb ? qr_sm_doubles(n, cb) : 0;
-    if (cb && q < MIX_SMEM_DOUBLES) q = MIX_SMEM_DOUBLES;
+    if (cb) q = q > MIX_SMEM_DOUBLES ? q : MIX_SMEM_DOUBLES;
     return smem_fixed(n) + (q > gu ? q : gu) + 8;
 }
 

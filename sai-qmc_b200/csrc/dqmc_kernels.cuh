@@ -318,9 +318,8 @@ __device__ __noinline__ int site_block(int n, int kb, int kbs, int i0, double *G
     double *facs = Tv + KB * LD;      /* fac_q                           */
     /* GEMM staging area, idle until the final flush: the staged block's
      * entries at this block ZA[a][k] = Zs_A[i0+a, k], YA[k][b] = Ys_A[k,
-     * i0+b] (row length LD), later -Pa^T and Qa (row length LT); TvP. */
-    double *ZA = s.gsm, *YA = s.gsm + KB * LT, *TvP = s.gsm + 2 * KB * LT;
-    double *TuP = Rrow;               /* Tu with row length LT, after the inverses */
+     * i0+b] (row length LD; block_flush reuses the area) */
+    double *ZA = s.gsm, *YA = s.gsm + KB * LT;
     int *alist = s.iscr;              /* accepted block positions, in order */
     /* two-spin path: G_down's records in the GEMM staging area (pairing is
      * off there, and the down spin is flushed first) */

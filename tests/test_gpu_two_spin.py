@@ -20,7 +20,7 @@ dq = pytest.importorskip("dqmc_b200")
 CASES = ["sq4_2spin", "chain3_2spin", "sq4_mu"]
 
 
-def engine_for(g, nbin=1):
+def engine_for(g, nbin=1, delay_rank=0):
     kind, Lx, Ly, L, stab, seed, sweeps, half, force = (int(x) for x in g["params"])
     if kind == 0:
         T, bp = dq.chain_lattice(Lx)
@@ -29,7 +29,7 @@ def engine_for(g, nbin=1):
             bp = None   # odd ring: not bipartite
     else:
         T, bp = dq.square_lattice(Lx, Ly)
-    eng = dq.Engine()
+    eng = dq.Engine(delay_rank=delay_rank)
     m = eng.add_model(T, bp, float(g["U"]), float(g["dtau"]), Lx, Ly,
                       mu=None if half else float(g["mu"]), two_spin=bool(force))
     eng.add_chain(m, L, stab, seed)
@@ -38,9 +38,12 @@ def engine_for(g, nbin=1):
 
 
 @pytest.mark.parametrize("name", CASES)
-def test_two_spin_matches_reference(name):
+@pytest.mark.parametrize("kb", [0, 1, 5])
+def test_two_spin_matches_reference(name, kb):
+    """kb: site-block size (0 = by n; 1 and 5 give several blocks, each
+    flushing both spins)."""
     g = golden(name)
-    eng, sweeps = engine_for(g, nbin=int(g["params"][6]))
+    eng, sweeps = engine_for(g, nbin=int(g["params"][6]), delay_rank=kb)
     np.testing.assert_array_equal(eng.field(0), g["field0"])
     assert np.max(np.abs(eng.green(0) - g["Gu0"])) < 1e-10
     assert np.max(np.abs(eng.green_down(0) - g["Gd0"])) < 1e-10
