@@ -41,6 +41,25 @@ def test_expm_matches_reference_model():
         assert rel_err(dq.expm_sym(K, float(g["dtau"])), g["expKinv"]) < 1e-13
 
 
+def test_expm_edge_cases():
+    """The host eigensolver behind the model exponential (Householder
+    tridiagonalization + implicit symmetric QR): sizes 1 and 2, a dense
+    random symmetric matrix, and a spectrum with repeated eigenvalues, each
+    against numpy's eigh; expK expK^-1 = I."""
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((50, 50))
+    blocks = np.kron(np.eye(5), np.ones((4, 4))) - 2.0 * np.eye(20)   # eigenvalues 2, -2 repeated
+    for K in (np.array([[0.7]]), np.array([[1.0, -0.5], [-0.5, 3.0]]), A + A.T, blocks,
+              np.zeros((6, 6))):
+        for sc in (-0.1, 0.25):
+            w, V = np.linalg.eigh(K)
+            want = (V * np.exp(sc * w)) @ V.T
+            got = dq.expm_sym(K, sc)
+            assert np.max(np.abs(got - want)) < 1e-12 * max(1.0, np.max(np.abs(want)))
+        E = dq.expm_sym(K, -0.1) @ dq.expm_sym(K, 0.1)
+        assert np.max(np.abs(E - np.eye(K.shape[0]))) < 1e-12
+
+
 def test_lattices_match_reference():
     for name in ("chain4_b2", "sq4_b4", "sq8_b4"):
         g = golden(name)
