@@ -271,15 +271,19 @@ int dqmc_expm_sym(int n, const double *A, double scale, double *out);
 
 /* No counterpart in the reference.  dqmc_udv_green for callers that must
  * not allocate device memory (their device memory is owned by their own
- * allocator, or they cannot afford the device-wide synchronization that
- * cudaMalloc/cudaFree can cause): the same arguments and result, computed
- * with a fixed scratch array inside the library instead of allocations.
- * n is limited to DQMC_NOALLOC_MAX_N; larger n is rejected with an error.
- * The array (about 1.1 MB) is held by every GPU that loads the library
- * until exit; the first call on a device also does that device's one-time
- * set-up, so make it before any stream capture on the device.  All calls
- * share the array: calls that overlap on the GPU race and must be
- * serialized by the caller. */
+ * allocator, e.g. a framework's caching pool that has reserved the GPU):
+ * the same arguments and result, computed with a fixed scratch array inside
+ * the library (about 1.1 MB) instead of allocations.  n is limited to
+ * DQMC_NOALLOC_MAX_N; larger n is rejected with an error.  The array and
+ * the kernel are placed on a device by the first call on that device (CUDA
+ * loads modules lazily), so that first call takes device memory and can
+ * fail for lack of it: make it before your allocator reserves the device,
+ * and before any stream capture on the device.  Later calls take no device
+ * memory; the array is held until the process exits.  A call selects
+ * `device`, runs on its legacy default stream, returns after the result is
+ * copied back, and restores the caller's current device.  All calls share
+ * the array: calls that overlap on the GPU race and must be serialized by
+ * the caller. */
 #define DQMC_NOALLOC_MAX_N 128
 int dqmc_udv_green_noalloc(int device, int n, const double *U, const double *D,
                            const double *T, double *G, int *det_sign);

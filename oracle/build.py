@@ -23,7 +23,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("SAIQMC_REF", "/root/reference")
+# The reference checkout: $SAIQMC_REF, else a "reference" directory beside
+# the repository root.
+REF = os.environ.get("SAIQMC_REF") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                  "reference")
 OUT = os.path.join(HERE, "_ref")
 
 

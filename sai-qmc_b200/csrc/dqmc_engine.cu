@@ -68,16 +68,16 @@ double host_rng_next(uint64_t *s)
     return (double)(res >> 11) * (1.0 / 9007199254740992.0);
 }
 
-/* Symmetric eigendecomposition by cyclic Jacobi rotations; A is overwritten
- * by its eigenvalues on the diagonal, V receives the eigenvectors. */
 /* Symmetric eigendecomposition A = Z diag(w) Z^T (column-major n x n), as
  * the reference's dsyev call in la_expm_sym (src/linalg.c:319-346) provides
  * it: Householder reduction to tridiagonal form with the reflectors
  * accumulated, then implicit symmetric QR steps with Wilkinson shifts on the
  * tridiagonal (Golub & Van Loan, Matrix Computations, Algorithms 5.1.1,
  * 8.3.1 and 8.3.2-8.3.3).  O(n^3) with a small constant: about 0.1 s at
- * n = 256 where cyclic Jacobi took seconds. */
-void sym_eig(int n, const double *A, std::vector<double> &w, std::vector<double> &Z)
+ * n = 256 where cyclic Jacobi took seconds.  Returns 0, or -1 when the QR
+ * iteration has not converged after 64 n shifts (w, Z are then not
+ * eigenpairs and must not be used). */
+int sym_eig(int n, const double *A, std::vector<double> &w, std::vector<double> &Z)
 {
     std::vector<double> a(A, A + (size_t)n * n);
     auto at = [&](int i, int j) -> double & { return a[i + (size_t)j * n]; };
@@ -177,6 +177,7 @@ void sym_eig(int n, const double *A, std::vector<double> &w, std::vector<double>
         }
     }
     w = d;
+    return q > 0 ? -1 : 0;
 }
 
 /* out_s = Z diag(exp(s_t w)) Z^T for the scales s_0, s_1 of one
@@ -285,7 +286,8 @@ int dqmc_expm_sym(int n, const double *A, double scale, double *out)
 {
     if (n <= 0 || !A || !out) return set_err("dqmc_expm_sym: bad arguments");
     std::vector<double> w, Z;
-    sym_eig(n, A, w, Z);
+    if (sym_eig(n, A, w, Z) != 0)
+        return set_err("dqmc_expm_sym: the symmetric QR iteration did not converge");
     expm_from_eig(n, w, Z, scale, out);
     return 0;
 }
@@ -387,7 +389,8 @@ int dqmc_model_add_mu(dqmc_engine *e, int n, int Lx, int Ly, const double *thop,
     m.expK.resize((size_t)n * n);
     m.expKinv.resize((size_t)n * n);
     std::vector<double> w, Z;   /* one decomposition for expK and expK^-1 */
-    sym_eig(n, K.data(), w, Z);
+    if (sym_eig(n, K.data(), w, Z) != 0)
+        return -set_err("dqmc_model_add: the eigensolver of t - mu I did not converge");
     expm_from_eig(n, w, Z, -dtau, m.expK.data());
     expm_from_eig(n, w, Z, dtau, m.expKinv.data());
     e->models.push_back(std::move(m));

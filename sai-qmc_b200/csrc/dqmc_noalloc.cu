@@ -4,23 +4,29 @@
  * out), for callers that must not allocate device memory: a host
  * application whose device memory is owned by its own allocator (a
  * framework's caching pool that has reserved the GPU, where an outside
- * cudaMalloc fails or fragments its pool), or a latency-critical caller for
- * which cudaMalloc/cudaFree -- which can synchronize the whole device --
- * are not acceptable.  Every buffer the kernel needs (the caller's U, D, T
- * staged on the device, the positive-D UDV slot, the QR workspaces, G and
- * the sign) lives in one file-scope __device__ array of fixed size for
- * n <= DQMC_NOALLOC_MAX_N (128): about 1.1 MB that every GPU which loads the
- * library keeps until the process exits.
+ * cudaMalloc fails or fragments its pool).  Every buffer the kernel needs
+ * (the caller's U, D, T staged on the device, the positive-D UDV slot, the
+ * QR workspaces, G and the sign) lives in one file-scope __device__ array
+ * of fixed size for n <= DQMC_NOALLOC_MAX_N (128), about 1.1 MB.
  *
- * The first call on a device looks up the device address of that array
- * (cudaGetSymbolAddress with that device current) and sets the kernel's
- * shared-memory limit; make that first call before any stream capture on
- * the device.  All calls share the one array and a call leaves its
- * contents behind: the sign slot is cleared at the start of every call and
- * everything else is written before it is read.  Two calls that overlap on
- * the GPU (from two host threads, for example) race on the array and must
- * be serialized by the caller.  No cudaMalloc, cudaFree or allocating
- * library routine is called, on the device or on the host.
+ * When that memory is taken: CUDA loads a module lazily (the default since
+ * CUDA 12.2), so the array and this file's kernel are placed on a device by
+ * the first call on that device, in its set-up (cudaGetSymbolAddress with
+ * the device current, and the kernel's shared-memory limit).  That first
+ * call can therefore fail for lack of device memory; make it before the
+ * caller's allocator reserves the device, and before any stream capture on
+ * the device.  Later calls take no device memory; the array stays until the
+ * process exits.
+ *
+ * The call selects `device`, runs on that device's legacy default stream
+ * with synchronous copies, returns only after the result has been copied
+ * back, and restores the caller's current device before it returns.  All
+ * calls share the one array and a call leaves its contents behind: the sign
+ * slot is cleared at the start of every call and everything else is written
+ * before it is read.  Two calls that overlap on the GPU (from two host
+ * threads, for example) race on the array and must be serialized by the
+ * caller.  No cudaMalloc, cudaFree or allocating library routine is called,
+ * on the device or on the host.
  */
 #define DQMC_NS dqn
 #include <cuda_runtime.h>
@@ -111,8 +117,29 @@ static int noalloc_fail(const char *msg, cudaError_t e)
     return 1;
 }
 
+/* Selects a device for the duration of one call and restores the caller's
+ * current device on every return path. */
+struct DeviceGuard {
+    int prev = -1;
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+static int noalloc_call(int device, int n, const double *U, const double *D, const double *T,
+                        double *G, int *det_sign);
+
 extern "C" int dqmc_udv_green_noalloc(int device, int n, const double *U, const double *D,
                                       const double *T, double *G, int *det_sign)
+{
+    DeviceGuard guard;
+    if (cudaGetDevice(&guard.prev) != cudaSuccess) guard.prev = -1;
+    return noalloc_call(device, n, U, D, T, G, det_sign);
+}
+
+static int noalloc_call(int device, int n, const double *U, const double *D, const double *T,
+                        double *G, int *det_sign)
 {
     if (!U || !D || !T || !G || !det_sign) return noalloc_fail("null argument", cudaSuccess);
     if (n <= 0 || n > NMAX) {

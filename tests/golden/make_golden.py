@@ -29,7 +29,9 @@ sys.path.insert(0, ROOT)
 from oracle import build as obuild  # noqa: E402
 from oracle.bind import LAT_CHAIN, LAT_SQUARE, Reference  # noqa: E402
 
-REF = os.environ.get("SAIQMC_REF", "/root/reference")
+# the reference checkout: $SAIQMC_REF, else a "reference" directory beside
+# the repository root (oracle/build.py uses the same rule)
+REF = obuild.REF
 
 # (name, kind, Lx, Ly, U, dtau, L, stab, seed, sweeps, selector)
 CASES = [
