@@ -248,10 +248,10 @@ def run_reference_arm(args):
 
 # ------------------------------------------------------------ GPU arm
 def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB, ctas_per_sm=0,
-                sweep_order=0):
+                sweep_order=0, green_log=0):
     T, bp = dq.square_lattice(LX, LX)
     eng = dq.Engine(device=device, precision=precision, delay_rank=delay_rank,
-                    ctas_per_sm=ctas_per_sm, sweep_order=sweep_order)
+                    ctas_per_sm=ctas_per_sm, sweep_order=sweep_order, green_log=green_log)
     m = eng.add_model(T, bp, U, DTAU, LX, LX, szz="af", sperp="af")
     for r in range(chains):
         eng.add_chain(m, L_SLICES, STAB, dq_replica_seed(SEED, 0, seed0 + r))
@@ -315,13 +315,42 @@ def e2e_run(steps, warmup, chains, precision):
                     "host<->device copies divided by its sweeps"}
 
 
+def lockstep_check(dq, nchains=4, sweeps=2):
+    """FP64 and mixed engines in lock step from the same seeds: field flips
+    compared, and max|G_mixed - G_FP64| of G as wrapped just before every
+    stabilization point (green_log snapshots; after a rebuild both are the
+    same FP64 function of the field), beside each mode's stabilization drift
+    max|G_wrapped - G_rebuilt| (the reference's drift diagnostic,
+    src/dqmc.c:64-98, on the engine's own rebuild)."""
+    M = -(-L_SLICES // STAB)
+    cap = M * sweeps + 2
+    ea = make_engine(dq, nchains, 0, dq.PREC_FP64, green_log=cap)
+    eb = make_engine(dq, nchains, 0, dq.PREC_MIXED, green_log=cap)
+    ea.prepare(1)
+    eb.prepare(1)
+    ea.sweep(sweeps)
+    eb.sweep(sweeps)
+    same = all(np.array_equal(ea.field(c), eb.field(c)) for c in range(nchains))
+    per_point = []
+    for c in range(nchains):
+        ga, gb = ea.green_log(c), eb.green_log(c)
+        k = min(len(ga), len(gb))
+        per_point += [float(np.max(np.abs(ga[i] - gb[i]))) for i in range(k)]
+    drift = {"fp64": max(ea.counters(c)["drift_max"] for c in range(nchains)),
+             "mixed": max(eb.counters(c)["drift_max"] for c in range(nchains))}
+    ea.close()
+    eb.close()
+    return {"chains": nchains, "sweeps": sweeps, "identical_flips": same,
+            "stabilization_points": len(per_point),
+            "max_dG_pre_rebuild": max(per_point) if per_point else None,
+            "median_dG_pre_rebuild": float(np.median(per_point)) if per_point else None,
+            "bound": 1e-8,
+            "stabilization_drift_max": drift}
+
+
 def precision_compare(dq, chains, args, precision, value):
     """The other precision mode on the same workload (same chains, warm-up
-    and timed sweeps), and a same-seed check between the two: 4 chains x 2
-    sweeps from identical fields, field flips compared, max|G_mixed -
-    G_FP64| after the sweeps (G is rebuilt from the FP64 stack at every
-    stabilization point) and each mode's stabilization drift
-    max|G_wrapped - G_rebuilt|."""
+    and timed sweeps), and the lock-step accuracy check."""
     other = dq.PREC_FP64 if precision == dq.PREC_MIXED else dq.PREC_MIXED
     e = make_engine(dq, chains, 0, other)
     e.prepare(1)
@@ -335,24 +364,12 @@ def precision_compare(dq, chains, args, precision, value):
     e.close()
     other_value = chains * N_SITES * L_SLICES / (ms * 1e-3)
     fp64_v, mixed_v = (value, other_value) if precision == dq.PREC_FP64 else (other_value, value)
-    ea = make_engine(dq, 4, 0, dq.PREC_FP64)
-    eb = make_engine(dq, 4, 0, dq.PREC_MIXED)
-    ea.prepare(1)
-    eb.prepare(1)
-    ea.sweep(2)
-    eb.sweep(2)
-    same = all(np.array_equal(ea.field(c), eb.field(c)) for c in range(4))
-    dg = max(float(np.max(np.abs(ea.green(c) - eb.green(c)))) for c in range(4))
-    drift = {"fp64": max(ea.counters(c)["drift_max"] for c in range(4)),
-             "mixed": max(eb.counters(c)["drift_max"] for c in range(4))}
-    ea.close()
-    eb.close()
     return {"fp64_value": fp64_v, "mixed_value": mixed_v, "mixed_over_fp64": mixed_v / fp64_v,
-            "mixed": "wrap products as 6-digit int8 split products (mma.sync s8), "
-                     "stabilization, B-blocks, flushes and ratios FP64",
-            "same_seed_check": {"chains": 4, "sweeps": 2, "identical_flips": same,
-                                "max_abs_dG_after_sweeps": dg,
-                                "stabilization_drift_max": drift}}
+            "target_ratio": 3.0,
+            "mixed": "wrap and delayed-update flush as FP64-emulated int8 split products "
+                     "(8 balanced base-256 digits per line, tcgen05.mma kind::i8, exact int32 "
+                     "accumulation in tensor memory); QR, G from UDV, B-blocks, ratios FP64",
+            "lockstep": lockstep_check(dq)}
 
 
 def alternating_order(dq, chains, args, precision, value):

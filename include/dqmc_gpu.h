@@ -27,6 +27,12 @@ extern "C" {
 
 typedef struct dqmc_engine dqmc_engine;
 
+/* FP64: every product in FP64 (DMMA tensor cores).  MIXED: the wrap
+ * (src/green.c:509-548) and the delayed-update flush (src/green.c:462-475)
+ * as FP64-emulated int8 split products on the tcgen05 tensor cores (8
+ * balanced base-256 digits per line, exact int32 accumulation); QR, G from
+ * UDV, B-block products, ratios and sign stay FP64.  Chain status bit 16
+ * (DQMC_ST_TIMEOUT) reports an abandoned split product. */
 enum { DQMC_PREC_FP64 = 0, DQMC_PREC_MIXED = 1 };
 /* Sweep order (DqmcSweepMode, src/dqmc.h:45-48): forward sweeps only, or
  * alternating forward / backward sweeps carrying the prefix and suffix UDV
@@ -85,7 +91,10 @@ enum {
 typedef struct {
     int device;      /* CUDA device ordinal                                  */
     int precision;   /* DQMC_PREC_*                                          */
-    int delay_rank;  /* site-block size k of the delayed update; 0 = by n    */
+    int delay_rank;  /* delay rank k of the delayed update (0 = 32): site
+                        blocks of k <= 32 sites; 32 < k <= 64 runs blocks
+                        of ceil(k/2) sites with paired G updates (one rank
+                        <= k update per k sites); k > 64 is rejected     */
     int drift;       /* bit-or of DQMC_DRIFT_*: STAB = max|G_wrap - G_stab|
                         at every stabilization (on by default); SCRATCH =
                         also the reference's rebuild-from-scratch drift
@@ -100,7 +109,14 @@ typedef struct {
                         the reference's udv_scale_file / udv_centered_file
                         diagnostics report (dqmc_read_udv_records); the
                         sweeps then run one launch per sweep             */
-    int reserved[3];
+    int green_log;   /* > 0: keep up to this many snapshots per chain of G as
+                        wrapped just before each stabilization point (the
+                        matrix the reference's drift diagnostic compares,
+                        src/dqmc.c:64-98), read with dqmc_read_green_log --
+                        e.g. two engines run in lock step from the same
+                        seeds give max|G_mixed - G_FP64| at every
+                        stabilization.  No counterpart in the reference.   */
+    int reserved[2];
 } dqmc_engine_desc;
 
 typedef struct {
@@ -287,6 +303,12 @@ int dqmc_expm_sym(int n, const double *A, double scale, double *out);
 #define DQMC_NOALLOC_MAX_N 128
 int dqmc_udv_green_noalloc(int device, int n, const double *U, const double *D,
                            const double *T, double *G, int *det_sign);
+
+/* Copies up to max_snapshots of a chain's G snapshots (n x n column-major
+ * each, in the order taken; see dqmc_engine_desc.green_log) to out and
+ * returns how many, or -1 on error; the log then restarts empty (snapshots
+ * beyond its capacity were not kept).  No counterpart in the reference. */
+int dqmc_read_green_log(dqmc_engine *e, int chain, double *out, int max_snapshots);
 
 /* Moves up to max_records of a chain's UDV scale records (in the order
  * they were taken, DQMC_UDV_RECORD_DOUBLES each) to out and returns how

@@ -52,12 +52,19 @@ def build(force=False, verbose=False):
                             "-I", os.path.join(ROOT, "include"), "-c", src, "-o",
                             obj], check=True)
             objs.append(obj)
-        cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17",
-               "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"),
-               "-o", LIB, *cu, *objs]
+        # the CUDA translation units compile in parallel (each takes minutes)
+        flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                 "-I", os.path.join(ROOT, "include")]
         if verbose:
-            cmd.append("-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+            flags.append("-Xptxas=-v")
+        procs, cobjs = [], []
+        for src in cu:
+            obj = os.path.join(bdir, os.path.basename(src) + ".o")
+            procs.append(subprocess.Popen([NVCC, *flags, "-c", src, "-o", obj]))
+            cobjs.append(obj)
+        if any([p.wait() != 0 for p in procs]):
+            raise subprocess.CalledProcessError(1, "nvcc")
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *cobjs, *objs], check=True)
     if main and (force or _stale(EXE, main + [LIB] + hdr)):
         subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Wextra",
                         "-I", os.path.join(ROOT, "include"), "-o", EXE, *main,

@@ -18,6 +18,7 @@
 #define DQMC_ST_SINGULAR 2   /* zero pivot in a QR                          */
 #define DQMC_ST_LOGRANGE 4   /* log-scale D left the representable range   */
 #define DQMC_ST_DETSIGN 8    /* det sign came out 0                         */
+#define DQMC_ST_TIMEOUT 16   /* a bounded wait on the tensor-core pipeline ran out */
 
 /* per-bin scalar accumulators (replica.h:6-16 ReplicaBin order)           */
 enum {
@@ -50,8 +51,25 @@ enum {
     DQMC_PH_COUNT
 };
 
-/* int8 digits per operand of a split product (42 bits) */
-#define DQMC_MIX_DIGITS 6
+/* int8 digits per operand of a split product (balanced base-256 digits,
+ * 8 S - 2 = 62 bits of each line's fixed-point representation) */
+#ifndef DQMC_MIX_DIGITS
+#define DQMC_MIX_DIGITS 8
+#endif
+/* pipeline stages of the split GEMM (shared memory: stages x digits x
+ * (128 + 128) lines x 32 bytes) */
+#ifndef DQMC_SPL_STAGES
+#define DQMC_SPL_STAGES 2
+#endif
+
+/* A split operand in device memory (dqmc_split.cuh): tiles (line block,
+ * k chunk) of DQMC_MIX_DIGITS digit slices in the tensor core's canonical
+ * layout, and one power-of-two scale per line. */
+typedef struct {
+    signed char *t;
+    double *sc;
+    int nlb, nkc;
+} DqmcSplitDev;
 
 typedef struct {
     int n, Lx, Ly;
@@ -67,12 +85,10 @@ typedef struct {
     const int *bipart;
     int nq_zz, nq_perp;
     const double *cos_zz, *cos_perp;   /* n x nq phase tables (structure_factor.c:182-199) */
-    /* split-product (mixed precision) operands: DQMC_MIX_DIGITS int8 digit
-     * slices of expK by rows ([i][k], ld mix_kp) and of expKinv by columns
-     * ([j][k]), with the power-of-two exponent of each row / column */
-    const signed char *mixK, *mixKinv;
-    const int *mixK_ex, *mixKinv_ex;
-    int mix_kp;
+    /* split-product (mixed precision) operands, precomputed per model:
+     * expK and expK^-1 by rows (A operands, 128-line blocks) and by
+     * columns (B operands, 64-line blocks) */
+    DqmcSplitDev spK_r, spK_c, spKi_r, spKi_c;
 } DqmcModelDev;
 
 typedef struct {
@@ -115,10 +131,13 @@ typedef struct {
     double *bins;              /* nbin x DQMC_BIN_FIELDS */
     double *bins_zz, *bins_perp;   /* nbin x nq */
     int nbin;
-    /* mixed precision: digit slices of one operand (DQMC_MIX_DIGITS x n x
-     * mix_kp bytes) and its n exponents; null in FP64 mode */
-    signed char *mix;
-    int *mix_ex;
+    /* mixed precision: the per-chain split buffers of an A operand (128-line
+     * blocks) and a B operand (64-line blocks) with K <= n; null in FP64 */
+    DqmcSplitDev spA, spB;
+    /* G as wrapped, before each rebuild (opt-in diagnostic): up to glog_cap
+     * snapshots of n x n, glog_n taken since the host last drained them */
+    double *glog;
+    int glog_cap, glog_n, glog_lost, glog_pad;
     unsigned long long prof[DQMC_PH_COUNT];
     /* calls of each phase's region as the reference's profiler counts them
      * (src/profiler.c): wraps, accepted flips and G updates, stack builds,

@@ -411,8 +411,10 @@ __device__ __forceinline__ void gemm_nn_rmw(int M, int N, int K, const double *A
  * small scratch.  cb is the widest of 64/48/32/16 that fits the CTA's
  * shared-memory budget; 0 selects the global-memory QR. */
 constexpr int QW = 20;              /* leading dimension of W (16 rows) */
-/* staging of the split-product GEMM (dqmc_mixed.cuh), one-CTA build only */
-constexpr size_t MIX_SMEM_DOUBLES = (DQMC_MINB == 1) ? 2560 * DQMC_MIX_DIGITS : 0;
+/* staging of the split-product GEMM (dqmc_split.cuh), one-CTA build only:
+ * DQMC_SPL_STAGES stages of DQMC_MIX_DIGITS x (128 + 128) lines x 32 bytes */
+constexpr size_t MIX_SMEM_DOUBLES =
+    (DQMC_MINB == 1) ? (size_t)DQMC_SPL_STAGES * DQMC_MIX_DIGITS * (128 + 128) * 32 / 8 : 0;
 constexpr size_t QR_MISC = 1920;    /* T, gram, taus, reductions        */
 constexpr size_t SMEM_BUDGET = (DQMC_MINB == 1 ? 227 * 1024 : 113 * 1024) / 8;
 
@@ -481,6 +483,7 @@ struct Smem {
     /* site-block view of the phase area */
     double *g0, *gt, *gam, *xs, *colA;
     QrSm q;          /* shared-memory QR view (overlaps gsm + phase) */
+    void *spl;       /* split-GEMM context (mixed precision), else null   */
 };
 
 __host__ __device__ inline size_t smem_doubles(int n, int kb)
@@ -530,6 +533,7 @@ __device__ inline Smem carve(double *base, int n, int kb)
     q.taus = q.gram + 256;
     q.rp = q.taus + 16;
     q.rf = q.rp + 16 * NW + NW + 8;
+    s.spl = nullptr;
     return s;
 }
 

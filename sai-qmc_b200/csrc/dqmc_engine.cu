@@ -211,6 +211,7 @@ struct HModel {
 
 struct HChain {
     int model, L, stab, M, kb;
+    int pair_forced;           /* delay rank > 32: two site blocks per G update */
     uint64_t rng[4];
     std::vector<signed char> field;
     std::vector<double> udv;   /* drained UDV scale records, oldest first */
@@ -438,9 +439,25 @@ int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
     c.L = L;
     c.stab = stab > 0 ? stab : 8;   /* green_stack_alloc default, src/green.c:172 */
     c.M = (L + c.stab - 1) / c.stab;
+    /* delay rank k: site blocks of k <= 32 sites (one register lane per
+     * column); 32 < k <= 64 runs blocks of ceil(k/2) sites whose G updates
+     * are paired, one rank <= k update per k sites */
     int kb = e->desc.delay_rank;
+    c.pair_forced = 0;
     if (kb <= 0) kb = 32;
-    if (kb > DQMC_MAX_KB) kb = DQMC_MAX_KB;
+    if (kb > 2 * DQMC_MAX_KB)
+        return -set_err("dqmc_chain_add: delay_rank %d exceeds %d (site blocks of at most %d "
+                        "sites, two per G update)", kb, 2 * DQMC_MAX_KB, DQMC_MAX_KB);
+    if (kb > DQMC_MAX_KB) {
+        if (e->desc.flush_pairs == DQMC_PAIRS_OFF)
+            return -set_err("dqmc_chain_add: delay_rank %d > %d needs paired flushes "
+                            "(flush_pairs is OFF)", kb, DQMC_MAX_KB);
+        if (!e->models[model].ph)
+            return -set_err("dqmc_chain_add: delay_rank %d > %d is not available on the "
+                            "two-spin path", kb, DQMC_MAX_KB);
+        kb = (kb + 1) / 2;
+        c.pair_forced = 1;
+    }
     if (kb > n) kb = n;
     c.kb = kb;
     uint64_t x = seed;
@@ -460,28 +477,36 @@ int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
     return (int)e->chains.size() - 1;
 }
 
-/* Digit slices of a split-product operand (the device's mix_split, same
- * arithmetic: X = trunc(x 2^(7S-e)) in base-128 digits, signed top digit): line l of M is row l (by_rows: M[l + k*n]) or column l
- * (M[k + l*n]); out: DQMC_MIX_DIGITS x n x kp bytes, ex: line exponents. */
-static void mix_split_host(int n, int kp, const double *M, bool by_rows,
-                           std::vector<signed char> &out, std::vector<int> &ex)
+/* A split-product operand of a model matrix (the device's spl_split, same
+ * arithmetic and block layout, dqmc_split.cuh): line l is row l of M
+ * (by_rows, M[l + k*n]) or column l (M[k + l*n]), in blocks of 128 lines;
+ * X = round(x 2^(NB - e)) in balanced base-256 digits (top digit first);
+ * sc[l] = 2^(e - NB + 4 (S - 1)). */
+static void split_host(int n, const double *M, bool by_rows, std::vector<signed char> &tiles,
+                       std::vector<double> &sc)
 {
-    out.assign((size_t)DQMC_MIX_DIGITS * n * kp, 0);
-    ex.assign(n, 0);
+    const int S = DQMC_MIX_DIGITS, NB = dq::SPL_NB, nkc = dq::spl_nkc(n);
+    tiles.assign(dq::spl_tile_bytes(n, n), 0);
+    sc.assign((size_t)dq::spl_nlb(n) * dq::SPL_LB, std::ldexp(1.0, -NB + 4 * (S - 1)));
     for (int l = 0; l < n; ++l) {
         auto val = [&](int k) { return by_rows ? M[l + (size_t)k * n] : M[k + (size_t)l * n]; };
         double m = 0.0;
         for (int k = 0; k < n; ++k) m = std::fmax(m, std::fabs(val(k)));
         int e = 0;
         if (m > 0.0) std::frexp(m, &e);
-        ex[l] = e;
-        const double sc = std::ldexp(1.0, 7 * DQMC_MIX_DIGITS - e);
+        sc[l] = std::ldexp(1.0, e - NB + 4 * (S - 1));
+        const double f = std::ldexp(1.0, NB - e);
         for (int k = 0; k < n; ++k) {
-            const long long X = (long long)(val(k) * sc);
-            for (int p = 0; p < DQMC_MIX_DIGITS; ++p) {
-                const int sh = 7 * (DQMC_MIX_DIGITS - 1 - p);
-                const unsigned d = p == 0 ? (unsigned)(X >> sh) & 255u : (unsigned)(X >> sh) & 127u;
-                out[(size_t)p * n * kp + (size_t)l * kp + k] = (signed char)(unsigned char)d;
+            long long X = std::llrint(val(k) * f);
+            for (int p = S - 1; p >= 0; --p) {
+                int d;
+                if (p > 0) {
+                    d = (int)((X + 128) & 255) - 128;
+                    X = (X - d) >> 8;
+                } else {
+                    d = (int)X;
+                }
+                tiles[dq::spl_offset(nkc, l, k, p)] = (signed char)d;
             }
         }
     }
@@ -512,22 +537,27 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
                 return set_err("dqmc_engine_prepare: mixed precision needs n <= %d here (n = %d)",
                                3 * DQMC_NT, m.n);
     }
+    /* split operands of a model: expK, expK^-1 by rows (A) and columns (B) */
+    auto spl_bytes = [](int n) {
+        return rup(dq::spl_tile_bytes(n, n)) + rup((size_t)dq::spl_nlb(n) * dq::SPL_LB * 8);
+    };
     size_t moff = 0;
     std::vector<size_t> mo(e->models.size() * 10);
     for (size_t k = 0; k < e->models.size(); ++k) {
         const HModel &m = e->models[k];
         const size_t nn = (size_t)m.n * m.n;
-        const size_t mixb = mixed ? (size_t)DQMC_MIX_DIGITS * m.n * dq::mix_kp(m.n) : 0;
         mo[10 * k + 0] = moff; moff += rup(nn * 8);
         mo[10 * k + 1] = moff; moff += rup(nn * 8);
         mo[10 * k + 2] = moff; moff += rup(nn * 8);
         mo[10 * k + 3] = moff; moff += rup((size_t)m.n * 4);
         mo[10 * k + 4] = moff; moff += rup(m.cos_zz.size() * 8 + 8);
         mo[10 * k + 5] = moff; moff += rup(m.cos_perp.size() * 8 + 8);
-        mo[10 * k + 6] = moff; moff += rup(mixb + 8);
-        mo[10 * k + 7] = moff; moff += rup(mixb + 8);
-        mo[10 * k + 8] = moff; moff += rup((size_t)m.n * 4);
-        mo[10 * k + 9] = moff; moff += rup((size_t)m.n * 4);
+        const size_t sa = mixed ? spl_bytes(m.n) : 0;
+        const size_t sb = sa;
+        mo[10 * k + 6] = moff; moff += sa;   /* expK by rows      */
+        mo[10 * k + 7] = moff; moff += sb;   /* expK by columns   */
+        mo[10 * k + 8] = moff; moff += sa;   /* expK^-1 by rows   */
+        mo[10 * k + 9] = moff; moff += sb;   /* expK^-1 by columns */
     }
     const size_t mstruct = moff;
     moff += rup(sizeof(DqmcModelDev) * e->models.size());
@@ -582,22 +612,23 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
             CU(cudaMemcpy(e->dmod + mo[10 * k + 5], m.cos_perp.data(), m.cos_perp.size() * 8,
                           cudaMemcpyHostToDevice));
         if (mixed) {
-            const int kp = dq::mix_kp(m.n);
-            std::vector<signed char> sl;
-            std::vector<int> ex;
-            d.mix_kp = kp;
-            d.mixK = (const signed char *)(e->dmod + mo[10 * k + 6]);
-            d.mixKinv = (const signed char *)(e->dmod + mo[10 * k + 7]);
-            d.mixK_ex = (const int *)(e->dmod + mo[10 * k + 8]);
-            d.mixKinv_ex = (const int *)(e->dmod + mo[10 * k + 9]);
-            mix_split_host(m.n, kp, m.expK.data(), true, sl, ex);
-            CU(cudaMemcpy(e->dmod + mo[10 * k + 6], sl.data(), sl.size(), cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(e->dmod + mo[10 * k + 8], ex.data(), ex.size() * 4,
-                          cudaMemcpyHostToDevice));
-            mix_split_host(m.n, kp, m.expKinv.data(), false, sl, ex);
-            CU(cudaMemcpy(e->dmod + mo[10 * k + 7], sl.data(), sl.size(), cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(e->dmod + mo[10 * k + 9], ex.data(), ex.size() * 4,
-                          cudaMemcpyHostToDevice));
+            std::vector<signed char> tl;
+            std::vector<double> sc;
+            auto put = [&](DqmcSplitDev &op, size_t off, const double *M, bool rows) -> int {
+                split_host(m.n, M, rows, tl, sc);
+                op.t = (signed char *)(e->dmod + off);
+                op.sc = (double *)(e->dmod + off + rup(tl.size()));
+                op.nlb = dq::spl_nlb(m.n);
+                op.nkc = dq::spl_nkc(m.n);
+                CU(cudaMemcpy(op.t, tl.data(), tl.size(), cudaMemcpyHostToDevice));
+                CU(cudaMemcpy(op.sc, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
+                return 0;
+            };
+            if (put(d.spK_r, mo[10 * k + 6], m.expK.data(), true) ||
+                put(d.spK_c, mo[10 * k + 7], m.expK.data(), false) ||
+                put(d.spKi_r, mo[10 * k + 8], m.expKinv.data(), true) ||
+                put(d.spKi_c, mo[10 * k + 9], m.expKinv.data(), false))
+                return 1;
         }
     }
     e->dmodels = (DqmcModelDev *)(e->dmod + mstruct);
@@ -634,10 +665,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += rup((size_t)e->nbin * DQMC_BIN_FIELDS * 8);
         off += rup((size_t)e->nbin * m.nq_zz * 8 + 8);
         off += rup((size_t)e->nbin * m.nq_perp * 8 + 8);
-        if (mixed) {
-            off += rup((size_t)DQMC_MIX_DIGITS * n * dq::mix_kp(n));   /* digit slices */
-            off += rup((size_t)n * 4);                                  /* exponents */
-        }
+        if (mixed) off += 2 * spl_bytes(n);
+        if (e->desc.green_log > 0) off += rup((size_t)e->desc.green_log * nn * 8);
         const size_t sm = dq::smem_bytes(n, c.kb);
         if (sm > maxsmem) maxsmem = sm;
         const size_t sm2 = dq2x::smem_bytes(n, c.kb);
@@ -672,7 +701,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         if (alt) d.P = (double *)take((size_t)(c.M + 1) * usz * 8);
         d.alt = alt ? 1 : 0;
         d.rebuild = e->desc.green_rebuild != DQMC_REBUILD_COMBINE ? 1 : 0;
-        d.pair = e->desc.flush_pairs == DQMC_PAIRS_ON ||
+        d.pair = c.pair_forced || e->desc.flush_pairs == DQMC_PAIRS_ON ||
                  (e->desc.flush_pairs == DQMC_PAIRS_AUTO && n >= 128);
         d.left = (double *)take(usz * 8);
         d.comb = (double *)take(usz * 8);
@@ -702,8 +731,17 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         d.bins_zz = (double *)take((size_t)e->nbin * m.nq_zz * 8 + 8);
         d.bins_perp = (double *)take((size_t)e->nbin * m.nq_perp * 8 + 8);
         if (mixed) {
-            d.mix = (signed char *)take((size_t)DQMC_MIX_DIGITS * n * dq::mix_kp(n));
-            d.mix_ex = (int *)take((size_t)n * 4);
+            for (int ab = 0; ab < 2; ++ab) {
+                DqmcSplitDev &op = ab ? d.spB : d.spA;
+                op.nlb = dq::spl_nlb(n);
+                op.nkc = dq::spl_nkc(n);
+                op.t = (signed char *)take(dq::spl_tile_bytes(n, n));
+                op.sc = (double *)take((size_t)op.nlb * dq::SPL_LB * 8);
+            }
+        }
+        if (e->desc.green_log > 0) {
+            d.glog_cap = e->desc.green_log;
+            d.glog = (double *)take((size_t)d.glog_cap * nn * 8);
         }
         CU(cudaMemcpy(d.field, c.field.data(), c.field.size(), cudaMemcpyHostToDevice));
     }
@@ -814,6 +852,44 @@ int dqmc_read_udv_records(dqmc_engine *e, int chain, double *out, int max_record
     const size_t nd = (size_t)k * DQMC_UDV_RECORD_DOUBLES;
     std::copy(h.begin(), h.begin() + nd, out);
     h.erase(h.begin(), h.begin() + nd);
+    return k;
+}
+
+int dqmc_read_green_log(dqmc_engine *e, int chain, double *out, int max_snapshots)
+{
+    if (chain_ok(e, chain, "dqmc_read_green_log")) return -1;
+    if (e->desc.green_log <= 0) {
+        set_err("dqmc_read_green_log: engine created without green_log");
+        return -1;
+    }
+    if (max_snapshots < 0 || (max_snapshots > 0 && !out)) {
+        set_err("dqmc_read_green_log: bad output buffer");
+        return -1;
+    }
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        set_err("dqmc_read_green_log: cudaStreamSynchronize");
+        return -1;
+    }
+    const DqmcChainDev &h = e->hdev[chain];
+    char *dc = (char *)(e->dchains + chain);
+    int cnt[2];   /* glog_cap, glog_n */
+    if (cudaMemcpy(cnt, dc + offsetof(DqmcChainDev, glog_cap), sizeof cnt,
+                   cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_err("dqmc_read_green_log: cudaMemcpy");
+        return -1;
+    }
+    const int k = cnt[1] < max_snapshots ? cnt[1] : max_snapshots;
+    const size_t nn = (size_t)h.n * h.n;
+    if (k > 0 && cudaMemcpy(out, h.glog, (size_t)k * nn * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_err("dqmc_read_green_log: cudaMemcpy");
+        return -1;
+    }
+    const int zero[2] = {0, 0};   /* glog_n, glog_lost */
+    if (cudaMemcpy(dc + offsetof(DqmcChainDev, glog_n), zero, sizeof zero,
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_err("dqmc_read_green_log: cudaMemcpy");
+        return -1;
+    }
     return k;
 }
 

@@ -2,7 +2,7 @@
 #pragma once
 #include "dqmc_device.cuh"
 #include "dqmc_gpu.h"
-#include "dqmc_mixed.cuh"
+#include "dqmc_split.cuh"
 
 namespace DQMC_NS {
 
@@ -64,6 +64,23 @@ __device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
  * facs: that spin's records; TuP: where Tu is laid out with even rows (the
  * spin's own Rrow area, free once the inverses exist).  Returns the staged
  * count left for the next block (0 after a G update). */
+/* G -= Zs Ys (rank mt): FP64 tiles, or the split product in mixed mode. */
+__device__ __forceinline__ void g_update(int n, int mt, double *G, const double *Zs,
+                                         const double *Ys, int ldy, const DqmcChainDev *ch,
+                                         Smem &s)
+{
+#if DQMC_MINB == 1
+    if (s.spl) {
+        flush_split(n, mt, G, Zs, Ys, ldy, ch, s);
+        return;
+    }
+#endif
+    (void)ch;
+    gemm_nn_rmw(
+        n, n, mt, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
+        [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
+}
+
 __device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G, double *Zs,
                                         double *Ys, int mA, bool flush, double *Rrow,
                                         double *Ccol, double *facs, double *TuP, Smem &s,
@@ -79,9 +96,7 @@ __device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G,
     const int ldy = 2 * kb;
     if (m == 0) {
         if (!flush || mA == 0) return mA;
-        gemm_nn_rmw(
-            n, n, mA, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
-            [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
+        g_update(n, mA, G, Zs, Ys, ldy, ch, s);
         pc.charge(ch, DQMC_PH_FLUSH, 1);
         return 0;
     }
@@ -290,9 +305,7 @@ __device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G,
         return mt;
     }
     /* G -= Zs Ys, rank mA + m */
-    gemm_nn_rmw(
-        n, n, mt, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
-        [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
+    g_update(n, mt, G, Zs, Ys, ldy, ch, s);
     pc.charge(ch, DQMC_PH_FLUSH, 1);
     return 0;
 }
@@ -588,6 +601,26 @@ __device__ __noinline__ void udv_record(DqmcChainDev *ch, int kind, int tau, int
     }
 }
 
+/* Snapshot of G as wrapped, just before a stabilization point replaces it
+ * (opt-in diagnostic: max|G_mixed - G_FP64| between engines run in lock
+ * step, and the wrapped G the reference's drift diagnostic compares,
+ * dqmc.c:64-98). */
+__device__ __noinline__ void glog_take(DqmcChainDev *ch, const double *G, int n)
+{
+    if (!ch->glog) return;
+    const int k = ch->glog_n;
+    if (k < ch->glog_cap) {
+        double *dst = ch->glog + (size_t)k * n * n;
+        ew_batched(n * n, [=](int e) { return G[e]; }, [=](int e, double x) { dst[e] = x; });
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (k < ch->glog_cap) ch->glog_n = k + 1;
+        else ch->glog_lost++;
+    }
+    __syncthreads();
+}
+
 /* The forward sweep, dqmc_sweep_forward (dqmc.c:609-813) with
  * carry_prefix = 0, use_ph = 1 and the combine rebuild.  Returns false on a
  * numerical failure (flag holds the reason). */
@@ -668,9 +701,9 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
         for (int q = 0; q < ns; ++q) {
             const Spin sp = spin_of(ch, md, q);
 #if DQMC_MINB == 1
-            if (kflags & KF_MIXED)
-                wrap_green_mixed(n, sp.G, tmp, md, fl, sp.v0, sp.v1, sp.vi0, sp.vi1, ch->mix,
-                                 ch->mix_ex, s);
+            if (s.spl)
+                wrap_green_split(n, sp.G, tmp, md, ch, fl, sp.v0, sp.v1, sp.vi0, sp.vi1, false,
+                                 s);
             else
 #endif
                 wrap_green(n, sp.G, tmp, md.expK, md.expKinv, fl, sp.v0, sp.v1, sp.vi0, sp.vi1,
@@ -748,6 +781,7 @@ __device__ __noinline__ bool sweep_body(DqmcChainDev *ch, const DqmcModelDev &md
             __syncthreads();
             if (*flag) return false;
             sgn *= ds;
+            if (q == 0) glog_take(ch, sp.G, n);
             const double dq = adopt_green(n, sp.G, Gn, s);
             /* a wrapped G that is not finite means the chain's state was lost
              * since the last rebuild: stop the chain (sticky status) */
@@ -809,8 +843,14 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     udv_identity(Sj(M), n);
     pc.charge(ch, DQMC_PH_STACK);
     auto back_wrap = [&](int l) {
-        wrap_green_back(n, G, tmp, md.expK, md.expKinv, ch->field + (size_t)l * n, v0, v1,
-                        md.expvinv[0], md.expvinv[1], s);
+#if DQMC_MINB == 1
+        if (s.spl)
+            wrap_green_split(n, G, tmp, md, ch, ch->field + (size_t)l * n, v0, v1,
+                             md.expvinv[0], md.expvinv[1], true, s);
+        else
+#endif
+            wrap_green_back(n, G, tmp, md.expK, md.expKinv, ch->field + (size_t)l * n, v0, v1,
+                            md.expvinv[0], md.expvinv[1], s);
         pc.charge(ch, DQMC_PH_WRAP, 1);
     };
     auto rebuild = [&](int tau, Udv u, bool boundary, int j) {
@@ -855,6 +895,7 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
         if (ds == 0) raise_flag(flag, DQMC_ST_DETSIGN);
         __syncthreads();
         if (*flag) return false;
+        glog_take(ch, G, n);
         const double d = adopt_green(n, G, Gn, s);
         /* a wrapped G that is not finite means the chain's state was lost
          * since the last rebuild: stop the chain (sticky status) */
@@ -897,6 +938,13 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     __syncthreads();
     if (flag) return;
     Smem s = carve(smraw, ch->n, ch->kb);
+#if DQMC_MINB == 1
+    __shared__ SplCtx spl;
+    if (kflags & KF_MIXED) {
+        spl_setup(&spl);
+        s.spl = &spl;
+    }
+#endif
     for (int sw = 0; sw < nsweeps; ++sw) {
         if (threadIdx.x == 0) {
             for (int i = 0; i < 4; ++i) rng[i] = ch->rng[i];
@@ -907,9 +955,16 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
         }
         __syncthreads();
         const bool back = ch->alt && ch->dir;
-        const bool ok = back ? sweep_body_back(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr)
-                             : sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
+        bool ok = back ? sweep_body_back(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr)
+                       : sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
         __syncthreads();
+#if DQMC_MINB == 1
+        if (s.spl && spl.err) {   /* a split product was abandoned */
+            ok = false;
+            if (threadIdx.x == 0) flag |= DQMC_ST_TIMEOUT;
+            __syncthreads();
+        }
+#endif
         if (threadIdx.x == 0) {
             for (int i = 0; i < 4; ++i) ch->rng[i] = rng[i];
             ch->attempts += att;
@@ -931,8 +986,11 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
             }
         }
         __syncthreads();
-        if (!ok || flag) return;
+        if (!ok || flag) break;
     }
+#if DQMC_MINB == 1
+    if (s.spl) spl_teardown(&spl);
+#endif
 }
 
 /* G from scratch at l0 = 0 for every chain (dqmc_init_modes, dqmc.c:466-483). */
@@ -1010,8 +1068,12 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     const int n = ch->n;
 #if DQMC_MINB == 1
     if (kflags & KF_MIXED) {
-        wrap_green_mixed(n, Gio, ch->w[4], md, ch->field + (size_t)l * n, md.expv[0], md.expv[1],
-                         md.expvinv[0], md.expvinv[1], ch->mix, ch->mix_ex, s);
+        __shared__ SplCtx spl;
+        spl_setup(&spl);
+        s.spl = &spl;
+        wrap_green_split(n, Gio, ch->w[4], md, ch, ch->field + (size_t)l * n, md.expv[0],
+                         md.expv[1], md.expvinv[0], md.expvinv[1], false, s);
+        spl_teardown(&spl);
         return;
     }
 #endif

@@ -41,7 +41,8 @@ class Desc(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int),
                 ("delay_rank", C.c_int), ("drift", C.c_int),
                 ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("green_rebuild", C.c_int),
-                ("flush_pairs", C.c_int), ("udv_diag", C.c_int), ("reserved", C.c_int * 3)]
+                ("flush_pairs", C.c_int), ("udv_diag", C.c_int), ("green_log", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class Counters(C.Structure):
@@ -113,6 +114,7 @@ def lib():
     L.dqmc_write_rng.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_uint64)]
     L.dqmc_expm_sym.argtypes = [C.c_int, _dp, C.c_double, _dp]
     L.dqmc_read_udv_records.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    L.dqmc_read_green_log.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
     L.dqmc_udv_green_noalloc.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                          C.POINTER(C.c_int)]
     _lib = L
@@ -205,7 +207,8 @@ class Engine:
 
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
                  drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD,
-                 green_rebuild=REBUILD_COMBINE, flush_pairs=PAIRS_AUTO, udv_diag=0):
+                 green_rebuild=REBUILD_COMBINE, flush_pairs=PAIRS_AUTO, udv_diag=0,
+                 green_log=0):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
@@ -215,6 +218,8 @@ class Engine:
         d.green_rebuild = green_rebuild
         d.flush_pairs = flush_pairs
         d.udv_diag = udv_diag
+        d.green_log = green_log
+        self.green_log_cap = green_log
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
             raise DqmcError(L.dqmc_last_error().decode())
@@ -319,6 +324,19 @@ class Engine:
         return (sc.reshape(self.nbin, NBIN_FIELDS),
                 zz[: self.nbin * m["nq_zz"]].reshape(self.nbin, m["nq_zz"]),
                 pp[: self.nbin * m["nq_perp"]].reshape(self.nbin, m["nq_perp"]))
+
+    def green_log(self, c):
+        """Snapshots of the chain's G as wrapped, just before each
+        stabilization point since the last call (needs green_log > 0):
+        array (k, n, n)."""
+        n = self.chains[c]["n"]
+        cap = max(1, self.green_log_cap)
+        buf = np.zeros(cap * n * n)
+        k = lib().dqmc_read_green_log(self.h, c, buf.ctypes.data, cap)
+        if k < 0:
+            raise DqmcError(lib().dqmc_last_error().decode())
+        return np.stack([_from_cm(buf[i * n * n:(i + 1) * n * n], n) for i in range(k)]) \
+            if k else np.zeros((0, n, n))
 
     def udv_records(self, c):
         """The chain's UDV scale records since the last call (needs

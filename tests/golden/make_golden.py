@@ -222,6 +222,76 @@ def two_spin(R):
         ch.free()
 
 
+# The batched uneven workload (dqmc_b200.workloads.uneven_batch, 64 chains of
+# 4x4..12x12 with drawn U and beta): a selection covering every lattice size,
+# each run by the reference on its own (beta index 0 keeps the seed), 2 sweeps
+# at stab 8.  And the large low-temperature lattice (workloads.LOWT, 24x24,
+# U=8, dtau=0.05): the full beta=10 (L=200) for one sweep, and a short L=40
+# for two sweeps.
+BATCH_SELECTION = (0, 6, 12, 18, 24, 33, 49, 63)
+BATCH_STAB, BATCH_SWEEPS = 8, 2
+
+
+def _g_summary(G):
+    """A full G for n <= 64; else its 32 x 32 corner, every 7th row/column
+    and its Frobenius norm (fixtures stay small)."""
+    n = G.shape[0]
+    if n <= 64:
+        return dict(G=G)
+    return dict(G_corner=G[:32, :32], G_sub=G[::7, ::7], G_fro=np.linalg.norm(G))
+
+
+def batches(R):
+    sys.path.insert(0, os.path.join(ROOT, "sai-qmc_b200"))
+    from dqmc_b200.workloads import LOWT, uneven_batch
+    chains = uneven_batch()
+    out = dict(selection=np.array(BATCH_SELECTION), stab=BATCH_STAB, sweeps=BATCH_SWEEPS)
+    for c in BATCH_SELECTION:
+        w = chains[c]
+        ch = R.chain(LAT_SQUARE, w["Lx"], w["Lx"], w["U"], w["dtau"], w["L"], BATCH_STAB,
+                     w["seed"], drift=True)
+        st0 = ch.state()
+        fields, cnt = [], []
+        for _ in range(BATCH_SWEEPS):
+            ch.sweep(1)
+            st = ch.state()
+            fields.append(st["field"])
+            cnt.append([st["attempts"], st["accepted"], st["sweeps"], st["status"]])
+        out[f"field0_{c}"] = st0["field"]
+        out[f"fields_{c}"] = np.array(fields)
+        out[f"counters_{c}"] = np.array(cnt, dtype=np.int64)
+        out[f"rng_{c}"] = st["rng"]
+        for k, v in _g_summary(st["Gu"]).items():
+            out[f"{k}_{c}"] = v
+        ch.free()
+    np.savez_compressed(os.path.join(HERE, "batch64_sel.npz"), **out)
+    w = LOWT
+    lo = {}
+    for tag, L, seed, sweeps in (("full", w["L"], w["seeds"][0], 1),
+                                 ("short", 40, w["seeds"][1], 2)):
+        ch = R.chain(LAT_SQUARE, w["Lx"], w["Lx"], w["U"], w["dtau"], L, w["stab"], seed,
+                     drift=True)
+        st0 = ch.state()
+        for k, v in _g_summary(st0["Gu"]).items():
+            lo[f"{tag}_{k}0"] = v
+        fields, cnt = [], []
+        for _ in range(sweeps):
+            ch.sweep(1)
+            st = ch.state()
+            fields.append(st["field"])
+            cnt.append([st["attempts"], st["accepted"], st["sweeps"], st["status"]])
+        lo[f"{tag}_params"] = np.array([w["Lx"], L, w["stab"], seed, sweeps], dtype=np.int64)
+        lo[f"{tag}_field0"] = st0["field"]
+        lo[f"{tag}_fields"] = np.array(fields)
+        lo[f"{tag}_counters"] = np.array(cnt, dtype=np.int64)
+        lo[f"{tag}_rng"] = st["rng"]
+        lo[f"{tag}_drift"] = R.drift(ch)
+        for k, v in _g_summary(st["Gu"]).items():
+            lo[f"{tag}_{k}"] = v
+        ch.free()
+    np.savez_compressed(os.path.join(HERE, "sq24_lowt.npz"), U=w["U"], dtau=w["dtau"], **lo)
+
+
 def headline_alt_fields():
     """Fields of the alternating headline chains, written as .npy to stdout."""
     R = Reference()
@@ -255,6 +325,10 @@ def main():
     if "--only-two-spin" in sys.argv:
         two_spin(R)
         print("wrote two-spin fixtures")
+        return
+    if "--only-batches" in sys.argv:
+        batches(R)
+        print("wrote batch64_sel.npz, sq24_lowt.npz")
         return
     if "--only-rebuild" in sys.argv:
         rebuild_modes(R)
@@ -325,6 +399,8 @@ def main():
     udv_fixture(os.path.join(HERE, "udv_fixture.npz"))
     alternating(R)
     rebuild_modes(R)
+    two_spin(R)
+    batches(R)
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 
