@@ -11,6 +11,9 @@ equal-time measurement.  value = whole-job field updates/s
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--chains B]
   python bench.py --impl reference ...   # the reference CPU code, host cores
+
+--gpus N > 1 without torchrun starts N ranks itself (one per GPU,
+dqmc_b200.launch); under torchrun each rank runs as started.
 """
 from __future__ import annotations
 
@@ -539,6 +542,10 @@ def main():
                     help="sweep kernel residency (0: automatic)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)   # at least three untimed steps
+    from dqmc_b200 import launch
+    if args.gpus > 1 and not launch.under_launcher():
+        # one rank per GPU, as torchrun would start them (rank 0 prints)
+        sys.exit(launch.main_self(args.gpus))
     if args.impl == "reference":
         run_reference_arm(args)
     else:

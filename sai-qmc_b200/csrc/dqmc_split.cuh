@@ -27,20 +27,25 @@
  * all 512 tensor-memory columns).
  *
  * Data path (one CTA = one chain, 256 threads):
- *  - operands are split into a tiled global buffer: tile (line block, k
- *    chunk) = S slices of LB lines x 32 bytes, each slice already in the
+ *  - operands are split into a tiled global buffer: block (128 lines, 32 k)
+ *    = S digit slices of 128 lines x 32 bytes, each slice already in the
  *    tensor core's K-major no-swizzle canonical layout (8-line x 16-byte
- *    core matrices; the two 16-byte k halves LB*16 bytes apart), so one
- *    pipeline stage of A (128 lines) or B (64 lines) is ONE contiguous bulk
- *    copy (cp.async.bulk, completing on an mbarrier);
- *  - thread 0 issues the copies (NSTAGE stages ahead) and, per 32-byte k
- *    chunk, the S(S+1)/2 tcgen05.mma (M = 128, N = 64, K = 32, s8 x s8 ->
- *    s32) into S accumulators of 64 tensor-memory columns each (S * 64 <=
- *    512), then tcgen05.commit to the stage's "empty" barrier;
- *  - after a tile's last chunk a commit to the "accum" barrier releases the
- *    epilogue: every warp reads its 32 tensor-memory lanes (tile rows) with
- *    tcgen05.ld, combines the S diagonals by Horner's rule in FP64 and
- *    scales by the two lines' powers of two.
+ *    core matrices; the two 16-byte k halves 2 KB apart), so the operand
+ *    data of one pipeline stage is one contiguous bulk copy per operand
+ *    (cp.async.bulk, completing on an mbarrier);
+ *  - output tiles are 128 x 128 (tcgen05.mma M = 128, N = 128, K = 32,
+ *    s8 x s8 -> s32) in two passes over k: pass 0 accumulates the digit
+ *    diagonals d = p + q = 0..3 (slices 0..3, 10 MMAs per chunk), pass 1
+ *    the diagonals 4..7 (26 MMAs), four accumulators of 128 tensor-memory
+ *    columns each.  A microbenchmark on B200 measured about 104 cycles per
+ *    M = 128 kind::i8 MMA for N <= 128 and 129 cycles for N = 256, so wide
+ *    tiles matter more than the number of accumulators;
+ *  - thread 0 issues the copies (one stage ahead) and the MMAs, then
+ *    tcgen05.commit to the stage's "empty" barrier and, after a pass's
+ *    last chunk, to the "accum" barrier that releases the epilogue: every
+ *    warp reads its 32 tensor-memory lanes (tile rows) with tcgen05.ld,
+ *    combines the pass's four diagonals exactly in int64 and scales by the
+ *    two lines' powers of two; pass 1 adds to pass 0's result.
  * Every wait is bounded (about two seconds); a wait that runs out sets the
  * context's error flag, the product is abandoned and the chain stops with
  * DQMC_ST_TIMEOUT.  Only the one-CTA-per-SM build carries this path (the
@@ -223,7 +228,7 @@ __device__ __forceinline__ void spl_tr4(uint32_t a, uint32_t b, uint32_t c, uint
 template <bool KCONTIG, class LD>
 __device__ __noinline__ void spl_split(int lines, int K, LD ld, SplitOp op)
 {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int lpad = op.nlb * SPL_LB;
     auto set_line = [&](int l, double m) {
         int e = 0;

@@ -241,6 +241,30 @@ def _g_summary(G):
     return dict(G_corner=G[:32, :32], G_sub=G[::7, ::7], G_fro=np.linalg.norm(G))
 
 
+def batch_fields():
+    """Fields of the selected batch chains after each sweep, as .npy on
+    stdout (run with another OPENBLAS_NUM_THREADS: a rounding variant of the
+    same reference)."""
+    sys.path.insert(0, os.path.join(ROOT, "sai-qmc_b200"))
+    from dqmc_b200.workloads import uneven_batch
+    R = Reference()
+    chains = uneven_batch()
+    out = []
+    for c in BATCH_SELECTION:
+        w = chains[c]
+        ch = R.chain(LAT_SQUARE, w["Lx"], w["Lx"], w["U"], w["dtau"], w["L"], BATCH_STAB,
+                     w["seed"], drift=True)
+        fr = []
+        for _ in range(BATCH_SWEEPS):
+            ch.sweep(1)
+            fr.append(ch.state()["field"].ravel())
+        out.append(np.concatenate(fr))
+        ch.free()
+    buf = io.BytesIO()
+    np.save(buf, np.concatenate(out))
+    sys.stdout.buffer.write(buf.getvalue())
+
+
 def batches(R):
     sys.path.insert(0, os.path.join(ROOT, "sai-qmc_b200"))
     from dqmc_b200.workloads import LOWT, uneven_batch
@@ -264,6 +288,17 @@ def batches(R):
         for k, v in _g_summary(st["Gu"]).items():
             out[f"{k}_{c}"] = v
         ch.free()
+    # the same chains with 4 BLAS threads: chain 24 (12x12, U=6, beta=10)
+    # meets an acceptance decision at the rounding level in its second sweep
+    # that the two thread counts take opposite ways; both are the reference's
+    var = subprocess.run([sys.executable, __file__, "--batch-fields"], check=True,
+                         capture_output=True, env=dict(os.environ, OPENBLAS_NUM_THREADS="4"))
+    flat = np.load(io.BytesIO(var.stdout))
+    off = 0
+    for c in BATCH_SELECTION:
+        sz = BATCH_SWEEPS * chains[c]["L"] * chains[c]["n"]
+        out[f"fields_t4_{c}"] = flat[off:off + sz].reshape(out[f"fields_{c}"].shape)
+        off += sz
     np.savez_compressed(os.path.join(HERE, "batch64_sel.npz"), **out)
     w = LOWT
     lo = {}
@@ -289,7 +324,33 @@ def batches(R):
         for k, v in _g_summary(st["Gu"]).items():
             lo[f"{tag}_{k}"] = v
         ch.free()
+        # the reference's own consistency at this point: its two-spin path
+        # builds G_down from the sigma = -1 factors, which must equal the
+        # particle-hole map I - P G_up^T P of G_up at half filling
+        cm = R.chain_mu(LAT_SQUARE, w["Lx"], w["Lx"], w["U"], w["dtau"], L, w["stab"], seed,
+                        half=True, two_spin=True)
+        sm = cm.state()
+        p = np.array([1.0 if ((i % w["Lx"]) + (i // w["Lx"])) % 2 == 0 else -1.0
+                      for i in range(w["Lx"] ** 2)])
+        lo[f"{tag}_ref_ph_violation0"] = float(np.max(np.abs(
+            sm["Gd"] - (np.eye(len(p)) - (p[:, None] * sm["Gu"].T) * p[None, :]))))
+        cm.free()
     np.savez_compressed(os.path.join(HERE, "sq24_lowt.npz"), U=w["U"], dtau=w["dtau"], **lo)
+
+
+def ed_table():
+    """Rows of the reference's exact-diagonalization table for the 4-site
+    U=4 chain (columns T, E_gc, C, N, Sz, S2, D_total, Z;
+    data/benchmark_L468_U4_full_diag_20260626/README.md) at the temperatures
+    the checks use."""
+    path = os.path.join(REF, "data", "benchmark_L468_U4_full_diag_20260626", "reference",
+                        "L4_U4_FullDiag.dat")
+    rows = np.array([[float(x) for x in l.split()] for l in open(path) if l.strip()])
+    want = [0.1, 0.15, 0.2, 0.25, 0.5, 1.0, 2.0]
+    sel = np.array([rows[np.argmin(np.abs(rows[:, 0] - T))] for T in want])
+    assert np.allclose(sel[:, 0], want)
+    np.savez_compressed(os.path.join(HERE, "ed_chain4_u4.npz"), T=sel[:, 0], E_gc=sel[:, 1],
+                        N=sel[:, 3], D_total=sel[:, 6], U=4.0, mu=2.0, L=4)
 
 
 def headline_alt_fields():
@@ -316,6 +377,9 @@ def main():
     if "--headline-alt-fields" in sys.argv:
         headline_alt_fields()
         return
+    if "--batch-fields" in sys.argv:
+        batch_fields()
+        return
     obuild.build_ref()
     R = Reference()
     if "--only-alternating" in sys.argv:
@@ -325,6 +389,10 @@ def main():
     if "--only-two-spin" in sys.argv:
         two_spin(R)
         print("wrote two-spin fixtures")
+        return
+    if "--only-ed" in sys.argv:
+        ed_table()
+        print("wrote ed_chain4_u4.npz")
         return
     if "--only-batches" in sys.argv:
         batches(R)
@@ -401,6 +469,7 @@ def main():
     rebuild_modes(R)
     two_spin(R)
     batches(R)
+    ed_table()
     print("wrote", sorted(f for f in os.listdir(HERE) if f.endswith(".npz")))
 
 

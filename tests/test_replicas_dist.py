@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 dq = pytest.importorskip("dqmc_b200")
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(dq.__file__)))
 from dqmc_b200 import replicas  # noqa: E402
 
 NREP, NBETA, NBIN = 5, 2, 3
@@ -81,3 +82,34 @@ def test_gather_layout_matches_ranges():
             first, count = replicas.rank_range(nrep, world, r)
             assert rc[r] == count * NBIN * dq.NBIN_FIELDS
             assert dp[r] == first * NBIN * dq.NBIN_FIELDS
+
+
+def test_spawn_local_runs_a_gloo_world_of_two(tmp_path):
+    """bench.py --gpus N spawns its own ranks when not under torchrun
+    (dqmc_b200.launch): the children get RANK/WORLD_SIZE/MASTER_* and form a
+    process group; rank 0's output comes back, the others' is dropped."""
+    import subprocess
+    import sys
+    script = tmp_path / "child.py"
+    script.write_text(
+        "import torch, torch.distributed as dist\n"
+        "dist.init_process_group('gloo')\n"
+        "t = torch.tensor([float(dist.get_rank() + 1)])\n"
+        "dist.all_reduce(t)\n"
+        "print('rank', dist.get_rank(), 'of', dist.get_world_size(), 'sum', int(t.item()))\n"
+        "dist.destroy_process_group()\n")
+    out = subprocess.run([sys.executable, "-c",
+                          "import sys; sys.path.insert(0, %r); from dqmc_b200 import launch; "
+                          "sys.exit(launch.spawn_local(2, [sys.executable, %r], timeout=120))"
+                          % (PKG, str(script))],
+                         capture_output=True, text=True, timeout=180)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "rank 0 of 2 sum 3"
+
+
+def test_spawn_local_reports_a_failing_rank(tmp_path):
+    import sys
+    from dqmc_b200 import launch
+    script = tmp_path / "fail.py"
+    script.write_text("import os, sys\nsys.exit(3 if os.environ['RANK'] == '1' else 0)\n")
+    assert launch.spawn_local(2, [sys.executable, str(script)], timeout=60) == 3
