@@ -375,6 +375,94 @@ def precision_compare(dq, chains, args, precision, value):
             "lockstep": lockstep_check(dq)}
 
 
+def batch_line(dq, kind, precision, sweeps, peak):
+    """One of the batched workloads as a sub-line: 'uneven' = the 64-chain
+    mix of 4x4..12x12 lattices with drawn U and beta (one launch per sweep,
+    bounded by its most expensive chain), 'lowt' = 8 chains of 24x24, U=8,
+    dtau=0.05, beta=10 (L=200), stab 5, delay rank 64.  Field updates/s over
+    timed sweeps after one untimed sweep, device-timed; roofline on the
+    chains' algorithmic FLOPs against the measured DGEMM peak."""
+    from dqmc_b200.workloads import LOWT, uneven_batch
+    if kind == "uneven":
+        chains = [dict(w, stab=8) for w in uneven_batch()]
+        eng = dq.Engine(precision=precision)
+    else:
+        chains = [dict(Lx=LOWT["Lx"], n=LOWT["Lx"] ** 2, U=LOWT["U"], dtau=LOWT["dtau"],
+                       L=LOWT["L"], stab=LOWT["stab"], seed=s) for s in LOWT["seeds"]]
+        eng = dq.Engine(precision=precision, delay_rank=LOWT["delay_rank"])
+    models = {}
+    for w in chains:
+        key = (w["Lx"], w["U"], w["dtau"])
+        if key not in models:
+            T, bp = dq.square_lattice(w["Lx"], w["Lx"])
+            models[key] = eng.add_model(T, bp, w["U"], w["dtau"], w["Lx"], w["Lx"])
+        eng.add_chain(models[key], w["L"], w["stab"], w["seed"])
+    t0 = time.perf_counter()
+    eng.prepare(1)
+    eng.sweep(1)
+    eng.sync()
+    setup_s = time.perf_counter() - t0
+    c0 = [eng.counters(c) for c in range(len(chains))]
+    eng.mark(0)
+    eng.sweep(sweeps)
+    eng.mark(1)
+    ms = eng.elapsed_ms() / sweeps
+    c1 = [eng.counters(c) for c in range(len(chains))]
+    eng.close()
+    upd = sum(w["n"] * w["L"] for w in chains)
+    flops = sum(flops_per_chain_sweep(w["n"], w["L"], w["stab"],
+                                      (c1[i]["accepted"] - c0[i]["accepted"]) / sweeps)
+                for i, w in enumerate(chains))
+    achieved = flops / (ms * 1e-3) / 1e12
+    crit = max(chains, key=lambda w: w["n"] ** 3 * w["L"])
+    return {"value": upd / (ms * 1e-3), "unit": UNIT, "ms_per_sweep": ms, "sweeps": sweeps,
+            "chains": len(chains), "field_updates_per_sweep": upd,
+            "precision": "mixed" if precision == dq.PREC_MIXED else "fp64",
+            "chains_failed": sum(1 for c in c1 if c["status"] != 0),
+            "setup_and_first_sweep_s": setup_s,
+            "critical_chain": {"n": crit["n"], "L": crit["L"]},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "flops_per_launch": flops}}
+
+
+def c3_sigma(dq, nwarm=100, nmeas=400, nbin=20):
+    """The single-chain 16x16 workload as specified (seed 11, nwarm 100,
+    nmeas 400, 20 bins) in FP64 and in mixed precision: each observable's
+    jackknife mean and error per mode, and |mean_mixed - mean_fp64| in units
+    of the FP64 error bar."""
+    out = {}
+    res = {}
+    for prec, name in ((dq.PREC_FP64, "fp64"), (dq.PREC_MIXED, "mixed")):
+        T, bp = dq.square_lattice(LX, LX)
+        e = dq.Engine(precision=prec, delay_rank=KB)
+        m = e.add_model(T, bp, U, DTAU, LX, LX, szz="af", sperp="af")
+        e.add_chain(m, L_SLICES, STAB, SEED)
+        e.prepare(nbin)
+        e.sweep(nwarm)
+        per = nmeas // nbin
+        for b in range(nbin):
+            e.sweep_measure(per, b)
+        sc, zz, pp = e.bins(0)
+        e.close()
+        sgn = sc[:, 5]
+        cols = {"E_hub": sc[:, 0] / sgn, "E_gc": sc[:, 1] / sgn, "n": sc[:, 3] / sgn,
+                "D": sc[:, 4] / sgn, "Szz_af": zz[:, 0] / sgn, "Sperp_af": pp[:, 0] / sgn}
+        res[name] = {}
+        for k, x in cols.items():
+            x = np.asarray(x)
+            loo = (x.sum() - x) / (len(x) - 1)
+            err = math.sqrt((len(x) - 1) / len(x) * np.sum((loo - loo.mean()) ** 2))
+            res[name][k] = (float(x.mean()), err)
+    for k in res["fp64"]:
+        m64, e64 = res["fp64"][k]
+        mmx, emx = res["mixed"][k]
+        out[k] = {"fp64": [m64, e64], "mixed": [mmx, emx],
+                  "diff_in_sigma": abs(mmx - m64) / e64 if e64 > 0 else None}
+    return {"workload": "16x16 U=4 beta=8, one chain, seed 11, nwarm 100, nmeas 400, 20 bins",
+            "observables": out}
+
+
 def alternating_order(dq, chains, args, precision, value):
     """The same workload in sweep_order=alternating (forward sweeps carrying
     the prefix stack, backward sweeps rebuilding the suffix stack): timed
@@ -444,6 +532,7 @@ def run_gpu_arm(args):
     accepted = sum(c1[i]["accepted"] - c0[i]["accepted"] for i in range(chains))
     attempts = sum(c1[i]["attempts"] - c0[i]["attempts"] for i in range(chains))
     drift = max(c["drift_max"] for c in c1)
+    drifts = np.array([c["drift_max"] for c in c1])
     ms_max = ms
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -495,9 +584,23 @@ def run_gpu_arm(args):
             "clocks": clocks,
             "acceptance": accepted / max(1, attempts),
             "drift_max": drift,
+            "drift": {"definition": "per chain, max|G_wrapped - G_rebuilt| over its "
+                                    "stabilization points in the timed sweeps",
+                      "median": float(np.median(drifts)),
+                      "p99": float(np.percentile(drifts, 99)), "max": float(drifts.max())},
             "chains_failed": status_bad,
             "measure_ms_per_step": meas_ms / max(1, nmeas),
         }
+        if world == 1 and not args.no_workloads:
+            line["workloads"] = {
+                "uneven_batch_64": {p: batch_line(dq, "uneven", pv, 3, peak)
+                                    for p, pv in (("fp64", dq.PREC_FP64),
+                                                  ("mixed", dq.PREC_MIXED))},
+                "lowt_24x24_beta10": {p: batch_line(dq, "lowt", pv, 1, peak)
+                                      for p, pv in (("fp64", dq.PREC_FP64),
+                                                    ("mixed", dq.PREC_MIXED))}}
+        if world == 1 and args.c3_sigma:
+            line["c3_sigma"] = c3_sigma(dq)
         if world == 1 and not args.no_compare:
             line["precision_compare"] = precision_compare(dq, chains, args, precision, value)
             line["alternating_order"] = alternating_order(dq, chains, args, precision, value)
@@ -538,6 +641,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-single-chain", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the uneven-batch and low-temperature sub-lines")
+    ap.add_argument("--c3-sigma", action="store_true",
+                    help="also run the single-chain 100/400/20 workload in both precisions "
+                         "and report each observable's difference in FP64 error bars")
     ap.add_argument("--ctas-per-sm", type=int, default=0, choices=[0, 1, 2],
                     help="sweep kernel residency (0: automatic)")
     args = ap.parse_args()

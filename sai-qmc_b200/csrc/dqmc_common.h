@@ -59,7 +59,7 @@ enum {
 /* pipeline stages of the split GEMM (shared memory: stages x digits x
  * (128 + 128) lines x 32 bytes) */
 #ifndef DQMC_SPL_STAGES
-#define DQMC_SPL_STAGES 2
+#define DQMC_SPL_STAGES 3
 #endif
 
 /* A split operand in device memory (dqmc_split.cuh): tiles (line block,
