@@ -173,10 +173,11 @@ def fp64_gemm_peak_tflops():
     return best
 
 
-def traffic_per_chain_sweep():
+def traffic_per_chain_sweep(mixed=False):
     """DRAM bytes per chain-sweep of the sweep kernel from the committed ncu
     summary (profiles/), or None when no capture has been summarized."""
-    path = os.path.join(ROOT, "profiles", "k_sweep_16x16_ncu.md")
+    path = os.path.join(ROOT, "profiles", "k_sweep_mixed_16x16_ncu.md" if mixed
+                        else "k_sweep_16x16_ncu.md")
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -555,7 +556,7 @@ def run_gpu_arm(args):
                 peak_src = "measured: cuBLAS DGEMM 8192^3 on this GPU (bench.py)"
             except Exception as exc:  # pragma: no cover
                 peak_src = f"nominal B200 FP64 tensor (DGEMM probe failed: {exc})"
-        tb = traffic_per_chain_sweep()
+        tb = traffic_per_chain_sweep(precision == dq.PREC_MIXED)
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak,
                     "unit": "TFLOP/s", "frac": achieved / peak,
                     "traffic": tb * chains if tb else None,

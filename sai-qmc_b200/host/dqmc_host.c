@@ -237,8 +237,8 @@ int dqmc_params_read(DqmcParams *p, const char *path)
                 tok = strtok(NULL, ",");
             }
         } else if (!strcmp(key, "delay_rank")) {
-            if (parse_int(val, &p->delay_rank) || p->delay_rank < 0 || p->delay_rank > 32)
-                FAIL("ERROR: delay_rank must be an integer in 0..32 (got %s)\n", val);
+            if (parse_int(val, &p->delay_rank) || p->delay_rank < 0 || p->delay_rank > 64)
+                FAIL("ERROR: delay_rank must be an integer in 0..64 (got %s)\n", val);
         } else if (!strcmp(key, "precision")) {
             if (strcmp(val, "fp64") && strcmp(val, "mixed"))
                 FAIL("ERROR: precision must be fp64 or mixed (got %s)\n", val);
