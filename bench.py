@@ -376,7 +376,7 @@ def precision_compare(dq, chains, args, precision, value):
             "lockstep": lockstep_check(dq)}
 
 
-def batch_line(dq, kind, precision, sweeps, peak):
+def batch_line(dq, kind, precision, sweeps, peak, tuned=False):
     """One of the batched workloads as a sub-line: 'uneven' = the 64-chain
     mix of 4x4..12x12 lattices with drawn U and beta (one launch per sweep,
     bounded by its most expensive chain), 'lowt' = 8 chains of 24x24, U=8,
@@ -384,8 +384,28 @@ def batch_line(dq, kind, precision, sweeps, peak):
     timed sweeps after one untimed sweep, device-timed; roofline on the
     chains' algorithmic FLOPs against the measured DGEMM peak."""
     from dqmc_b200.workloads import LOWT, uneven_batch
+    tuning = None
     if kind == "uneven":
         chains = [dict(w, stab=8) for w in uneven_batch()]
+        if tuned:
+            # per size class: delay rank, flush grouping and interval
+            # (the workload leaves n_wrap to the tuner), dqmc_b200.autotune
+            from dqmc_b200 import autotune
+            keys = sorted({(w["Lx"], w["L"], w["U"]) for w in chains})
+            classes = [dict(Lx=Lx, Ly=Lx, n=Lx * Lx, L=L, U=U_, dtau=DTAU, stab=8)
+                       for Lx, L, U_ in keys]
+            t0 = time.perf_counter()
+            tuner = autotune.Tuner()
+            picks = dict(zip(keys, tuner.tune(classes, tune_stab=True)))
+            tuning = {"seconds": time.perf_counter() - t0, "trials": tuner.trials,
+                      "classes": len(keys),
+                      "choices": {f"{Lx}x{Lx} L={L} U={U_:g}": {k: p[k] for k in
+                                  ("delay_rank", "flush_pairs", "stab")}
+                                  for (Lx, L, U_), p in picks.items()}}
+            for w in chains:
+                p = picks[(w["Lx"], w["L"], w["U"])]
+                w.update(stab=p["stab"], delay_rank=p["delay_rank"],
+                         flush_pairs=p["flush_pairs"])
         eng = dq.Engine(precision=precision)
     else:
         chains = [dict(Lx=LOWT["Lx"], n=LOWT["Lx"] ** 2, U=LOWT["U"], dtau=LOWT["dtau"],
@@ -397,7 +417,9 @@ def batch_line(dq, kind, precision, sweeps, peak):
         if key not in models:
             T, bp = dq.square_lattice(w["Lx"], w["Lx"])
             models[key] = eng.add_model(T, bp, w["U"], w["dtau"], w["Lx"], w["Lx"])
-        eng.add_chain(models[key], w["L"], w["stab"], w["seed"])
+        cid = eng.add_chain(models[key], w["L"], w["stab"], w["seed"])
+        if "delay_rank" in w:
+            eng.tune_chain(cid, w["delay_rank"], w["flush_pairs"])
     t0 = time.perf_counter()
     eng.prepare(1)
     eng.sweep(1)
@@ -416,7 +438,7 @@ def batch_line(dq, kind, precision, sweeps, peak):
                 for i, w in enumerate(chains))
     achieved = flops / (ms * 1e-3) / 1e12
     crit = max(chains, key=lambda w: w["n"] ** 3 * w["L"])
-    return {"value": upd / (ms * 1e-3), "unit": UNIT, "ms_per_sweep": ms, "sweeps": sweeps,
+    line = {"value": upd / (ms * 1e-3), "unit": UNIT, "ms_per_sweep": ms, "sweeps": sweeps,
             "chains": len(chains), "field_updates_per_sweep": upd,
             "precision": "mixed" if precision == dq.PREC_MIXED else "fp64",
             "chains_failed": sum(1 for c in c1 if c["status"] != 0),
@@ -425,6 +447,9 @@ def batch_line(dq, kind, precision, sweeps, peak):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "flops_per_launch": flops}}
+    if tuning:
+        line["autotune"] = tuning
+    return line
 
 
 def c3_sigma(dq, nwarm=100, nmeas=400, nbin=20):
@@ -594,9 +619,10 @@ def run_gpu_arm(args):
         }
         if world == 1 and not args.no_workloads:
             line["workloads"] = {
-                "uneven_batch_64": {p: batch_line(dq, "uneven", pv, 3, peak)
-                                    for p, pv in (("fp64", dq.PREC_FP64),
-                                                  ("mixed", dq.PREC_MIXED))},
+                "uneven_batch_64": dict(
+                    {p: batch_line(dq, "uneven", pv, 3, peak)
+                     for p, pv in (("fp64", dq.PREC_FP64), ("mixed", dq.PREC_MIXED))},
+                    fp64_tuned=batch_line(dq, "uneven", dq.PREC_FP64, 3, peak, tuned=True)),
                 "lowt_24x24_beta10": {p: batch_line(dq, "lowt", pv, 1, peak)
                                       for p, pv in (("fp64", dq.PREC_FP64),
                                                     ("mixed", dq.PREC_MIXED))}}

@@ -181,9 +181,18 @@ int dqmc_model_set_spin(dqmc_engine *e, int model, int nq_zz, const int *mx_zz,
 int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
                    const signed char *field);
 
+/* Sets one chain's delay rank and flush grouping (dqmc_engine_desc's
+ * delay_rank and flush_pairs apply to every chain otherwise), before
+ * dqmc_engine_prepare: an autotuner gives each size class of a batch its
+ * own.  The accept/reject sequence is the same for every setting.  No
+ * counterpart in the reference (its delay rank is fixed at 16,
+ * src/green.c:10). */
+int dqmc_chain_tune(dqmc_engine *e, int chain, int delay_rank, int flush_pairs);
+
 /* Allocates device state for all chains, uploads models and fields and
  * builds each chain's G from scratch (green_from_scratch, src/green.c:262).
- * nbin measurement bins are reserved per chain. */
+ * nbin measurement bins are reserved per chain.  Sweeps launch the chains
+ * most expensive first (cost n^3 L). */
 int dqmc_engine_prepare(dqmc_engine *e, int nbin);
 
 /* Advances every healthy chain by nsweeps forward sweeps (dqmc_sweep,

@@ -212,6 +212,7 @@ struct HModel {
 struct HChain {
     int model, L, stab, M, kb;
     int pair_forced;           /* delay rank > 32: two site blocks per G update */
+    int pair_mode;             /* DQMC_PAIRS_* of this chain                   */
     uint64_t rng[4];
     std::vector<signed char> field;
     std::vector<double> udv;   /* drained UDV scale records, oldest first */
@@ -238,6 +239,7 @@ struct dqmc_engine {
     char *dmod = nullptr, *darena = nullptr;
     DqmcModelDev *dmodels = nullptr;
     DqmcChainDev *dchains = nullptr;
+    int *dorder = nullptr;           /* launch order of the sweep kernel */
     std::vector<DqmcChainDev> hdev;  /* host mirror: device pointers */
     int nbin = 0;
     size_t smem = 0, msmem = 0, smem2 = 0;
@@ -427,6 +429,45 @@ int dqmc_model_set_spin(dqmc_engine *e, int model, int nq_zz, const int *mx_zz,
     return 0;
 }
 
+/* Delay rank k of one chain: site blocks of k <= 32 sites (one register
+ * lane per column); 32 < k <= 64 runs blocks of ceil(k/2) sites whose G
+ * updates are paired, one rank <= k update per k sites. */
+static int set_delay(dqmc_engine *e, HChain &c, int n, int model, int delay_rank, int pairs,
+                     const char *who)
+{
+    int kb = delay_rank;
+    c.pair_forced = 0;
+    if (pairs < DQMC_PAIRS_AUTO || pairs > DQMC_PAIRS_ON)
+        return set_err("%s: flush_pairs %d is not a DQMC_PAIRS_* value", who, pairs);
+    c.pair_mode = pairs;
+    if (kb <= 0) kb = 32;
+    if (kb > 2 * DQMC_MAX_KB)
+        return set_err("%s: delay_rank %d exceeds %d (site blocks of at most %d sites, two per "
+                       "G update)", who, kb, 2 * DQMC_MAX_KB, DQMC_MAX_KB);
+    if (kb > DQMC_MAX_KB) {
+        if (pairs == DQMC_PAIRS_OFF)
+            return set_err("%s: delay_rank %d > %d needs paired flushes (flush_pairs is OFF)",
+                           who, kb, DQMC_MAX_KB);
+        if (!e->models[model].ph)
+            return set_err("%s: delay_rank %d > %d is not available on the two-spin path", who,
+                           kb, DQMC_MAX_KB);
+        kb = (kb + 1) / 2;
+        c.pair_forced = 1;
+    }
+    if (kb > n) kb = n;
+    c.kb = kb;
+    return 0;
+}
+
+int dqmc_chain_tune(dqmc_engine *e, int chain, int delay_rank, int flush_pairs)
+{
+    if (!e || e->prepared || chain < 0 || chain >= (int)e->chains.size())
+        return set_err("dqmc_chain_tune: bad engine/chain, or engine already prepared");
+    HChain &c = e->chains[chain];
+    return set_delay(e, c, e->models[c.model].n, c.model, delay_rank, flush_pairs,
+                     "dqmc_chain_tune");
+}
+
 int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
                    const signed char *field)
 {
@@ -439,27 +480,8 @@ int dqmc_chain_add(dqmc_engine *e, int model, int L, int stab, uint64_t seed,
     c.L = L;
     c.stab = stab > 0 ? stab : 8;   /* green_stack_alloc default, src/green.c:172 */
     c.M = (L + c.stab - 1) / c.stab;
-    /* delay rank k: site blocks of k <= 32 sites (one register lane per
-     * column); 32 < k <= 64 runs blocks of ceil(k/2) sites whose G updates
-     * are paired, one rank <= k update per k sites */
-    int kb = e->desc.delay_rank;
-    c.pair_forced = 0;
-    if (kb <= 0) kb = 32;
-    if (kb > 2 * DQMC_MAX_KB)
-        return -set_err("dqmc_chain_add: delay_rank %d exceeds %d (site blocks of at most %d "
-                        "sites, two per G update)", kb, 2 * DQMC_MAX_KB, DQMC_MAX_KB);
-    if (kb > DQMC_MAX_KB) {
-        if (e->desc.flush_pairs == DQMC_PAIRS_OFF)
-            return -set_err("dqmc_chain_add: delay_rank %d > %d needs paired flushes "
-                            "(flush_pairs is OFF)", kb, DQMC_MAX_KB);
-        if (!e->models[model].ph)
-            return -set_err("dqmc_chain_add: delay_rank %d > %d is not available on the "
-                            "two-spin path", kb, DQMC_MAX_KB);
-        kb = (kb + 1) / 2;
-        c.pair_forced = 1;
-    }
-    if (kb > n) kb = n;
-    c.kb = kb;
+    if (set_delay(e, c, n, model, e->desc.delay_rank, e->desc.flush_pairs, "dqmc_chain_add"))
+        return -1;
     uint64_t x = seed;
     for (int i = 0; i < 4; ++i) c.rng[i] = splitmix(&x);
     c.field.resize((size_t)L * n);
@@ -675,6 +697,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     }
     const size_t cstruct = off;
     off += rup(sizeof(DqmcChainDev) * nc);
+    const size_t corder = off;
+    off += rup(sizeof(int) * nc);
     CU(cudaMalloc(&e->darena, off));
     CU(cudaMemset(e->darena, 0, off));
     e->hdev.assign(nc, DqmcChainDev());
@@ -701,8 +725,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         if (alt) d.P = (double *)take((size_t)(c.M + 1) * usz * 8);
         d.alt = alt ? 1 : 0;
         d.rebuild = e->desc.green_rebuild != DQMC_REBUILD_COMBINE ? 1 : 0;
-        d.pair = c.pair_forced || e->desc.flush_pairs == DQMC_PAIRS_ON ||
-                 (e->desc.flush_pairs == DQMC_PAIRS_AUTO && n >= 128);
+        d.pair = c.pair_forced || c.pair_mode == DQMC_PAIRS_ON ||
+                 (c.pair_mode == DQMC_PAIRS_AUTO && n >= 128);
         d.left = (double *)take(usz * 8);
         d.comb = (double *)take(usz * 8);
         d.scr = (double *)take(usz * 8);
@@ -748,6 +772,21 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     e->dchains = (DqmcChainDev *)(e->darena + cstruct);
     CU(cudaMemcpy(e->dchains, e->hdev.data(), sizeof(DqmcChainDev) * nc,
                   cudaMemcpyHostToDevice));
+    /* sweep launch order: most expensive chain first (a sweep costs about
+     * n^3 L, twice that on the two-spin path), ties in insertion order */
+    {
+        std::vector<int> order(nc);
+        for (size_t k = 0; k < nc; ++k) order[k] = (int)k;
+        auto cost = [&](int k) {
+            const HChain &c = e->chains[k];
+            const HModel &m = e->models[c.model];
+            return (double)m.n * m.n * m.n * c.L * (m.ph ? 1.0 : 2.0);
+        };
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return cost(a) > cost(b); });
+        e->dorder = (int *)(e->darena + corder);
+        CU(cudaMemcpy(e->dorder, order.data(), sizeof(int) * nc, cudaMemcpyHostToDevice));
+    }
     e->smem = maxsmem;
     e->msmem = (size_t)2 * maxn * 8;
     if (e->smem > 227 * 1024) return set_err("shared memory need %zu B exceeds 227 KB", e->smem);
@@ -825,9 +864,11 @@ int dqmc_sweep(dqmc_engine *e, int nsweeps)
     for (int done = 0; done < nsweeps; done += per) {
         ev_begin(e, 0);
         if (e->per_sm == 2)
-            dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), per);
+            dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), per,
+                                 e->dorder);
         else
-            dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, kflags(e), per);
+            dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, kflags(e), per,
+                               e->dorder);
         ev_end(e);
         CU(cudaGetLastError());
         if (udv_drain(e)) return 1;
@@ -902,9 +943,9 @@ int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
         const int f = kflags(e) | dq::KF_MEASURE;
         ev_begin(e, 0);
         if (e->per_sm == 2)
-            dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, f, 1);
+            dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, f, 1, e->dorder);
         else
-            dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, f, 1);
+            dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, f, 1, e->dorder);
         ev_end(e);
         if (udv_drain(e)) return 1;
         ev_begin(e, 1);

@@ -13,9 +13,9 @@ namespace dq2x {
 size_t smem_bytes(int n, int kb) { return dq2::smem_bytes(n, kb); }
 cudaError_t set_attrs(size_t smem, size_t msmem) { return dq2::set_attrs(smem, msmem); }
 void launch_sweep(unsigned nc, size_t smem, cudaStream_t st, DqmcChainDev *c,
-                  const DqmcModelDev *m, int flags, int nsweeps)
+                  const DqmcModelDev *m, int flags, int nsweeps, const int *order)
 {
-    dq2::launch_sweep(nc, smem, st, c, m, flags, nsweeps);
+    dq2::launch_sweep(nc, smem, st, c, m, flags, nsweeps, order);
 }
 void launch_measure(unsigned nc, size_t msmem, cudaStream_t st, DqmcChainDev *c,
                     const DqmcModelDev *m, int bin)

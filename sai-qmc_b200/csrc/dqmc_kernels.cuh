@@ -925,14 +925,17 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     return rebuild(0, left, false, 0);
 }
 
+/* One CTA per chain; order[b] names the chain of block b (longest first,
+ * so a batch of uneven chains does not end on a late-starting long one). */
 __global__ void __launch_bounds__(NT, DQMC_MINB)
-    k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps)
+    k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps,
+            const int *order)
 {
     extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     __shared__ uint64_t rng[4];
     __shared__ unsigned long long att, acc;
-    DqmcChainDev *ch = &chains[blockIdx.x];
+    DqmcChainDev *ch = &chains[order ? order[blockIdx.x] : blockIdx.x];
     const DqmcModelDev &md = models[ch->model];
     if (threadIdx.x == 0) flag = ch->status;
     __syncthreads();
@@ -1246,9 +1249,9 @@ inline cudaError_t set_attrs(size_t smem, size_t msmem)
 }
 
 inline void launch_sweep(unsigned nc, size_t smem, cudaStream_t st, DqmcChainDev *c,
-                         const DqmcModelDev *m, int flags, int nsweeps)
+                         const DqmcModelDev *m, int flags, int nsweeps, const int *order)
 {
-    k_sweep<<<nc, NT, smem, st>>>(c, m, flags, nsweeps);
+    k_sweep<<<nc, NT, smem, st>>>(c, m, flags, nsweeps, order);
 }
 
 inline void launch_measure(unsigned nc, size_t msmem, cudaStream_t st, DqmcChainDev *c,

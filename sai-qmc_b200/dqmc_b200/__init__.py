@@ -87,6 +87,7 @@ def lib():
     L.dqmc_chain_add.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                  C.c_uint64, C.c_void_p]
     L.dqmc_engine_prepare.argtypes = [C.c_void_p, C.c_int]
+    L.dqmc_chain_tune.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.dqmc_sweep.argtypes = [C.c_void_p, C.c_int]
     L.dqmc_sweep_measure.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.dqmc_synchronize.argtypes = [C.c_void_p]
@@ -264,6 +265,10 @@ class Engine:
             raise DqmcError(lib().dqmc_last_error().decode())
         self.chains.append(dict(model=model, n=self.models[model]["n"], L=L))
         return cid
+
+    def tune_chain(self, c, delay_rank, flush_pairs=PAIRS_AUTO):
+        """Per-chain delay rank and flush grouping (before prepare)."""
+        _check(lib().dqmc_chain_tune(self.h, c, delay_rank, flush_pairs), "chain_tune")
 
     def prepare(self, nbin=1):
         self.nbin = nbin
