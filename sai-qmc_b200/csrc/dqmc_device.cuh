@@ -1274,6 +1274,50 @@ __device__ void qr_store_rows_t(QrSm &q, int n, double *M, int r0, int nr, const
     __syncthreads();
 }
 
+/* Applies reflector panels p0 = first, first + step, ... (count panels) of
+ * a factored A to the active block: apply(p0) runs qr_apply_sm on the
+ * staged panel.  While panel p0 is applied, the next panel's reflector
+ * rows and compact-WY factor are already loading into registers (one row
+ * of 16 per thread), so the global-memory latency of the staging overlaps
+ * the products; the staged values equal qr_load_v's.  Panels taller than
+ * the CTA stage through qr_load_v. */
+template <class F>
+__device__ __forceinline__ void qr_panels(QrSm &q, int n, const double *A, const double *tw,
+                                          int first, int step, int count, F apply)
+{
+    if (count <= 0) return;
+    const int lo = step > 0 ? first : first + step * (count - 1);
+    if (((n - lo + 15) & ~15) > NT) {
+        for (int i = 0; i < count; ++i) {
+            const int p0 = first + i * step;
+            qr_load_v(q, n, A, tw, p0);
+            apply(p0);
+        }
+        return;
+    }
+    const int r = threadIdx.x, ld = q.ld;
+    double v[16], t = 0.0;
+    auto fetch = [&](int p0) {
+        const int m = n - p0, nb = min(16, m);
+        const double *src = A + p0 + (size_t)p0 * n;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = (c < nb && r < m && r > c) ? src[r + (size_t)c * n] : 0.0;
+        if (r < 256) t = tw[(size_t)(p0 / 16) * 256 + r];
+    };
+    fetch(first);
+    for (int i = 0; i < count; ++i) {
+        const int p0 = first + i * step, m = n - p0, nb = min(16, m), R = (m + 15) & ~15;
+        if (r < R) {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) q.V[r + c * ld] = (r == c && c < nb) ? 1.0 : v[c];
+        }
+        if (r < 256) q.T[r] = t;
+        __syncthreads();
+        if (i + 1 < count) fetch(p0 + step);
+        apply(p0);
+    }
+}
+
 __device__ __noinline__ int qr_factor_sm(int n, double *A, double *tw, Smem &s, int *flag)
 {
     QrSm &q = s.q;
@@ -1282,10 +1326,8 @@ __device__ __noinline__ int qr_factor_sm(int n, double *A, double *tw, Smem &s, 
     for (int jb = 0; jb < n; jb += cb) {
         const int nc = min(cb, n - jb);
         qr_load_cols(q, n, A, jb, nc);
-        for (int p0 = 0; p0 < jb; p0 += 16) {
-            qr_load_v(q, n, A, tw, p0);
-            qr_apply_sm(q, q.X + p0, n - p0, nc, true);
-        }
+        qr_panels(q, n, A, tw, 0, 16, jb / 16,
+                  [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nc, true); });
         for (int pc = 0; pc < nc; pc += 16) {
             const int j0 = jb + pc, m = n - j0, nb = min(16, m);
             double *Xp = q.X + j0 + (size_t)pc * ld;
@@ -1317,10 +1359,9 @@ __device__ __noinline__ void qr_form_q_sm(int n, const double *A, const double *
             for (int r = threadIdx.x; r < R; r += NT)
                 q.X[r + (size_t)c * ld] = (c < nc && r == jb + c) ? 1.0 : 0.0;
         __syncthreads();
-        for (int p0 = ((jb + nc - 1) / 16) * 16; p0 >= 0; p0 -= 16) {
-            qr_load_v(q, n, A, tw, p0);
-            qr_apply_sm(q, q.X + p0, n - p0, nc, false);
-        }
+        const int top = ((jb + nc - 1) / 16) * 16;
+        qr_panels(q, n, A, tw, top, -16, top / 16 + 1,
+                  [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nc, false); });
         qr_store_cols(q, n, Q, jb, nc);
     }
 }
@@ -1333,10 +1374,8 @@ __device__ __noinline__ void qr_apply_qt_sm(int n, const double *A, const double
     for (int jb = 0; jb < ncols; jb += q.cb) {
         const int nc = min(q.cb, ncols - jb);
         qr_load_cols(q, n, Y, jb, nc);
-        for (int p0 = 0; p0 < n; p0 += 16) {
-            qr_load_v(q, n, A, tw, p0);
-            qr_apply_sm(q, q.X + p0, n - p0, nc, true);
-        }
+        qr_panels(q, n, A, tw, 0, 16, (n + 15) / 16,
+                  [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nc, true); });
         qr_store_cols(q, n, Y, jb, nc);
     }
 }
@@ -1351,10 +1390,8 @@ __device__ __noinline__ void qr_apply_right_sm(int n, const double *A, const dou
     for (int r0 = 0; r0 < n; r0 += q.cb) {
         const int nr = min(q.cb, n - r0);
         qr_load_rows_t(q, n, Xin, r0, nr);
-        for (int p0 = 0; p0 < n; p0 += 16) {
-            qr_load_v(q, n, A, tw, p0);
-            qr_apply_sm(q, q.X + p0, n - p0, nr, true);
-        }
+        qr_panels(q, n, A, tw, 0, 16, (n + 15) / 16,
+                  [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nr, true); });
         qr_store_rows_t(q, n, Xout, r0, nr, cs);
     }
 }
