@@ -42,6 +42,8 @@ UNIT = "field updates/s"
 LX, U, DTAU, BETA, STAB, KB, SEED = 16, 4.0, 0.1, 8.0, 8, 32, 11
 N_SITES = LX * LX
 L_SLICES = int(round(BETA / DTAU))
+INT8_DENSE_OPS = 4.5e15   # nominal dense int8 tensor rate of a B200
+SM_MAX_MHZ = 1965
 L2_BYTES = 126 * 2**20
 
 
@@ -361,10 +363,30 @@ def precision_compare(dq, chains, args, precision, value):
     for _ in range(args.warmup):
         e.sweep(1)
     e.sync()
+    p0 = [e.profile(c) for c in range(chains)] if other == dq.PREC_MIXED else None
     e.mark(0)
     e.sweep(args.steps)
     e.mark(1)
     ms = e.elapsed_ms() / args.steps
+    split = None
+    if p0 is not None:
+        p1 = [e.profile(c) for c in range(chains)]
+        wrap_cyc = sum(p1[c]["wrap"] - p0[c]["wrap"] for c in range(chains)) / (chains * args.steps)
+        flush_cyc = sum(p1[c]["flush"] - p0[c]["flush"] for c in range(chains)) / (chains * args.steps)
+        # one split product of n x n by n x n: 36 digit products (p + q <= 7 of
+        # 8 digits), n^3 int8 multiply-adds each; the wrap is two per slice
+        ops = 2 * L_SLICES * 36 * 2 * N_SITES ** 3
+        import torch
+        nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        peak = INT8_DENSE_OPS / (nsm * SM_MAX_MHZ * 1e6)
+        split = {"phase": "wrap (both split products and their digit splits and epilogues)",
+                 "bound": "tensor (int8)", "int8_ops_per_chain_sweep": ops,
+                 "wrap_cycles_per_chain_sweep": wrap_cyc,
+                 "flush_cycles_per_chain_sweep": flush_cyc,
+                 "achieved_ops_per_cycle_per_sm": ops / wrap_cyc,
+                 "peak_ops_per_cycle_per_sm": peak, "frac": ops / wrap_cyc / peak,
+                 "peak_source": "nominal dense int8 4.5 POPS / (SMs x 1965 MHz); one chain "
+                                "per SM, phase clocks of each chain"}
     e.close()
     other_value = chains * N_SITES * L_SLICES / (ms * 1e-3)
     fp64_v, mixed_v = (value, other_value) if precision == dq.PREC_FP64 else (other_value, value)
@@ -373,6 +395,7 @@ def precision_compare(dq, chains, args, precision, value):
             "mixed": "wrap and delayed-update flush as FP64-emulated int8 split products "
                      "(8 balanced base-256 digits per line, tcgen05.mma kind::i8, exact int32 "
                      "accumulation in tensor memory); QR, G from UDV, B-blocks, ratios FP64",
+            "split_roofline": split,
             "lockstep": lockstep_check(dq)}
 
 
@@ -585,6 +608,10 @@ def run_gpu_arm(args):
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak,
                     "unit": "TFLOP/s", "frac": achieved / peak,
                     "traffic": tb * chains if tb else None,
+                    "traffic_gbs": tb * chains / (avg_launch * 1e-3) / 1e9 if tb else None,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                      "k_sweep launch of 296 chains (profiles/), per chain-sweep "
+                                      "x chains",
                     "kernel": "k_sweep (one launch = one sweep of every chain)",
                     "flops_per_launch": flops_launch,
                     "flops_definition": "algorithmic F(measured acceptance) per chain-sweep "
