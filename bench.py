@@ -275,7 +275,7 @@ def dq_replica_seed(base, b, r):
     return lib.dqmc_replica_seed(base, b, r)
 
 
-def e2e_run(steps, warmup, chains, precision):
+def e2e_run(steps, warmup, chains, precision, device=0, seed=None):
     """The user-facing call end to end: dqmc_host_run on an input file for the
     same workload (host parsing, model exponential, uploads of the model and
     of every chain's field, initial G, warm-up and measured sweeps, read-back
@@ -289,7 +289,8 @@ def e2e_run(steps, warmup, chains, precision):
     nmeas = nbin * max(1, math.ceil(steps / nbin))
     text = (f"lattice=square\nLx={LX}\nLy={LX}\nbc=periodic\nt=-1.0\nU={U}\ndtau={DTAU}\n"
             f"beta_list={BETA}\nstab={STAB}\nnwarm={warmup}\nnmeas={nmeas}\nnbin={nbin}\n"
-            f"nrep={chains}\nseed={SEED}\ndelay_rank={KB}\nprecision={precision}\n"
+            f"nrep={chains}\nseed={SEED if seed is None else seed}\ndelay_rank={KB}\n"
+            f"precision={precision}\ngpu_device={device}\n"
             f"replica_log=none\nszz_q=af\nsperp_q=af\n")
     cwd = os.getcwd()
     with tempfile.TemporaryDirectory() as d:
@@ -461,12 +462,30 @@ def batch_line(dq, kind, precision, sweeps, peak, tuned=False):
                 for i, w in enumerate(chains))
     achieved = flops / (ms * 1e-3) / 1e12
     crit = max(chains, key=lambda w: w["n"] ** 3 * w["L"])
+    crit_line = {"n": crit["n"], "L": crit["L"]}
+    if not tuned and (kind == "uneven" or precision == dq.PREC_FP64):
+        # the most expensive chain alone: a launch of one chain per CTA
+        # cannot take less than this chain's own sweep
+        e1 = dq.Engine(precision=precision,
+                       delay_rank=LOWT["delay_rank"] if kind == "lowt" else 0)
+        T, bp = dq.square_lattice(crit["Lx"], crit["Lx"])
+        m1 = e1.add_model(T, bp, crit["U"], crit["dtau"], crit["Lx"], crit["Lx"])
+        e1.add_chain(m1, crit["L"], crit["stab"], crit["seed"])
+        e1.prepare(1)
+        e1.sweep(1)
+        e1.sync()
+        e1.mark(0)
+        e1.sweep(sweeps)
+        e1.mark(1)
+        alone = e1.elapsed_ms() / sweeps
+        e1.close()
+        crit_line.update(ms_per_sweep_alone=alone, batch_over_alone=ms / alone)
     line = {"value": upd / (ms * 1e-3), "unit": UNIT, "ms_per_sweep": ms, "sweeps": sweeps,
             "chains": len(chains), "field_updates_per_sweep": upd,
             "precision": "mixed" if precision == dq.PREC_MIXED else "fp64",
             "chains_failed": sum(1 for c in c1 if c["status"] != 0),
             "setup_and_first_sweep_s": setup_s,
-            "critical_chain": {"n": crit["n"], "L": crit["L"]},
+            "critical_chain": crit_line,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "flops_per_launch": flops}}
@@ -590,6 +609,21 @@ def run_gpu_arm(args):
     value = world * chains * N_SITES * L_SLICES * args.steps / (ms_max * 1e-3)
     eng.close()
 
+    # end to end through the public entry point on every rank (its own
+    # device and seeds), the slowest rank's wall time
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        r = e2e_run(args.steps, args.warmup, chains, args.precision, device=local,
+                    seed=SEED + 1000 * rank)
+        dt = r["seconds"] if r else float("inf")
+        if world > 1:
+            t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        if r and math.isfinite(dt):
+            e2e = dict(r, value=world * r["value"] * r["seconds"] / dt, seconds=dt)
+
     if rank == 0:
         acc_per_chain_sweep = accepted / max(1, chains * args.steps)
         flops_launch = chains * flops_per_chain_sweep(N_SITES, L_SLICES, STAB, acc_per_chain_sweep)
@@ -670,8 +704,8 @@ def run_gpu_arm(args):
             e1.close()
             line["single_chain"] = {"value": N_SITES * L_SLICES / (t1 * 1e-3), "unit": UNIT,
                                     "ms_per_sweep": t1}
-        if not args.no_e2e and world == 1:
-            line["e2e"] = e2e_run(args.steps, args.warmup, chains, args.precision)
+        if e2e is not None:
+            line["e2e"] = e2e
         if not args.no_cpu_baseline and world == 1:
             cb = reference_cpu(2, 0)
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
