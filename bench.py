@@ -254,10 +254,11 @@ def run_reference_arm(args):
 
 # ------------------------------------------------------------ GPU arm
 def make_engine(dq, chains, seed0, precision, device=0, delay_rank=KB, ctas_per_sm=0,
-                sweep_order=0, green_log=0):
+                sweep_order=0, green_log=0, chain_ctas=0):
     T, bp = dq.square_lattice(LX, LX)
     eng = dq.Engine(device=device, precision=precision, delay_rank=delay_rank,
-                    ctas_per_sm=ctas_per_sm, sweep_order=sweep_order, green_log=green_log)
+                    ctas_per_sm=ctas_per_sm, sweep_order=sweep_order, green_log=green_log,
+                    chain_ctas=chain_ctas)
     m = eng.add_model(T, bp, U, DTAU, LX, LX, szz="af", sperp="af")
     for r in range(chains):
         eng.add_chain(m, L_SLICES, STAB, dq_replica_seed(SEED, 0, seed0 + r))
@@ -455,6 +456,7 @@ def batch_line(dq, kind, precision, sweeps, peak, tuned=False):
     eng.mark(1)
     ms = eng.elapsed_ms() / sweeps
     c1 = [eng.counters(c) for c in range(len(chains))]
+    chain_ctas = eng.residency()[1]
     eng.close()
     upd = sum(w["n"] * w["L"] for w in chains)
     flops = sum(flops_per_chain_sweep(w["n"], w["L"], w["stab"],
@@ -478,12 +480,15 @@ def batch_line(dq, kind, precision, sweeps, peak, tuned=False):
         e1.sweep(sweeps)
         e1.mark(1)
         alone = e1.elapsed_ms() / sweeps
+        alone_ctas = e1.residency()[1]
         e1.close()
-        crit_line.update(ms_per_sweep_alone=alone, batch_over_alone=ms / alone)
+        crit_line.update(ms_per_sweep_alone=alone, batch_over_alone=ms / alone,
+                         chain_ctas_alone=alone_ctas)
     line = {"value": upd / (ms * 1e-3), "unit": UNIT, "ms_per_sweep": ms, "sweeps": sweeps,
             "chains": len(chains), "field_updates_per_sweep": upd,
             "precision": "mixed" if precision == dq.PREC_MIXED else "fp64",
             "chains_failed": sum(1 for c in c1 if c["status"] != 0),
+            "chain_ctas": chain_ctas,
             "setup_and_first_sweep_s": setup_s,
             "critical_chain": crit_line,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
@@ -693,17 +698,24 @@ def run_gpu_arm(args):
             line["precision_compare"] = precision_compare(dq, chains, args, precision, value)
             line["alternating_order"] = alternating_order(dq, chains, args, precision, value)
         if not args.no_single_chain and world == 1:
-            e1 = make_engine(dq, 1, 0, precision)
-            e1.prepare(1)
-            e1.sweep(1)
-            e1.sync()
-            e1.mark(0)
-            e1.sweep(2)
-            e1.mark(1)
-            t1 = e1.elapsed_ms() / 2
-            e1.close()
+            # one chain: a thread-block cluster per chain (automatic size)
+            # and, for comparison, one CTA per chain; same trajectory
+            single = {}
+            for key, cc in (("cluster", 0), ("one_cta", 1)):
+                e1 = make_engine(dq, 1, 0, precision, chain_ctas=cc)
+                e1.prepare(1)
+                e1.sweep(1)
+                e1.sync()
+                e1.mark(0)
+                e1.sweep(2)
+                e1.mark(1)
+                single[key] = (e1.elapsed_ms() / 2, e1.residency()[1])
+                e1.close()
+            t1, cc1 = single["cluster"]
             line["single_chain"] = {"value": N_SITES * L_SLICES / (t1 * 1e-3), "unit": UNIT,
-                                    "ms_per_sweep": t1}
+                                    "ms_per_sweep": t1, "chain_ctas": cc1,
+                                    "one_cta_ms_per_sweep": single["one_cta"][0],
+                                    "over_one_cta": single["one_cta"][0] / t1}
         if e2e is not None:
             line["e2e"] = e2e
         if not args.no_cpu_baseline and world == 1:

@@ -116,7 +116,21 @@ typedef struct {
                         e.g. two engines run in lock step from the same
                         seeds give max|G_mixed - G_FP64| at every
                         stabilization.  No counterpart in the reference.   */
-    int reserved[2];
+    int chain_ctas;  /* CTAs that advance one chain together as a thread-block
+                        cluster, 2..16 (above 8 where the device allows a
+                        non-portable cluster size); 1 = one CTA per chain;
+                        0 = automatic: for FP64 batches of fewer chains
+                        than SMs with a lattice of n >= 128, the largest
+                        size at which all the batch's clusters are resident
+                        at once, else 1.  Rank 0 runs the sweep; every rank
+                        forms its share of the output tiles of the wrap,
+                        the B-block products and the delayed-update G
+                        update, so the trajectory equals the one-CTA run
+                        bit for bit.  For batches of fewer chains than SMs
+                        (one chain, a few large lattices).  FP64 only; one
+                        CTA per SM.  No counterpart in the reference, whose
+                        sweep runs on one host thread.                       */
+    int reserved;
 } dqmc_engine_desc;
 
 typedef struct {
@@ -222,6 +236,10 @@ int dqmc_synchronize(dqmc_engine *e);
 
 int dqmc_chain_count(const dqmc_engine *e);
 int dqmc_chain_dims(const dqmc_engine *e, int chain, int *n, int *L);
+/* The sweep kernel's residency chosen at dqmc_engine_prepare: chains per
+ * SM (1 or 2) and CTAs per chain (1, or the cluster size).  No counterpart
+ * in the reference. */
+int dqmc_engine_residency(const dqmc_engine *e, int *ctas_per_sm, int *chain_ctas);
 
 /* Copies back the up-spin G (n x n) at the chain's current slice (0 after a
  * sweep).  G_down = I - P G_up^T P (src/green.c:372-382). */

@@ -91,6 +91,18 @@ typedef struct {
     DqmcSplitDev spK_r, spK_c, spKi_r, spKi_c;
 } DqmcModelDev;
 
+/* Command block of a chain advanced by a thread-block cluster: rank 0
+ * writes the product the cluster forms next (op, operands, sizes, scalars);
+ * the other ranks read it after the cluster barrier. */
+typedef struct {
+    int op, i[3];
+    const void *p[6];
+    double d[4];
+} DqmcClCmd;
+
+/* largest cluster that advances one chain (non-portable size above 8)     */
+#define DQMC_MAX_CHAIN_CTAS 16
+
 typedef struct {
     int model, n, L, stab, M, kb;
     int status, bvalid;        /* bvalid: cached B-block products are current */
@@ -144,6 +156,7 @@ typedef struct {
      * B-block products, UDV updates, combines, G from UDV, adoptions,
      * rebuilds from scratch, measurements */
     unsigned long long pcalls[DQMC_PH_COUNT];
+    DqmcClCmd cl;
 } DqmcChainDev;
 
 /* UDV slot: U (n*n) | T (n*n) | ell = log D (n) | detU (1) | pad (1)        */

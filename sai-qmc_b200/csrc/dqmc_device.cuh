@@ -163,10 +163,19 @@ struct Ident {
     __device__ __forceinline__ double operator()(int, int, double x) const { return x; }
 };
 
-template <class T, bool AMF, bool BKF, bool RMW, class LA, class LB, class LC, class ST,
-          class SA = Ident, class SB = Ident>
+/* Share of a product's output tiles taken by one CTA: tiles r, r + c,
+ * r + 2c, ... of the column-major tile grid.  {0, 1} is the whole product;
+ * the CTAs of a cluster that advance one chain together take {rank, size}.
+ * Every output element is formed by the same instruction sequence whatever
+ * the share, so a split product equals the unsplit one bit for bit. */
+struct Part {
+    int r = 0, c = 1;
+};
+
+template <class T, bool AMF, bool BKF, bool RMW, bool PART = false, class LA, class LB, class LC,
+          class ST, class SA = Ident, class SB = Ident>
 __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, double *sm,
-                          SA sa = SA(), SB sb = SB())
+                          SA sa = SA(), SB sb = SB(), Part pt = Part())
 {
     constexpr int BM = T::BM, BN = T::BN, BK = T::BK, TM = T::TM, TN = T::TN;
     constexpr int TX = T::TX, TY = T::TY, AP = T::AP, BP = T::BP;
@@ -178,8 +187,9 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
     const int wm = warp % T::WM, wn = warp / T::WM;
     const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN;
     const int nk = (K + BK - 1) / BK;
-    const int total = tm * tn * nk;
-    (void)tn;
+    const int ntile = tm * tn;
+    const int mine = !PART ? ntile : ntile > pt.r ? (ntile - pt.r + pt.c - 1) / pt.c : 0;
+    const int total = mine * nk;
     /* output coordinates of accumulator (r, c) of this thread in a tile */
     auto out_ij = [&](int r, int c, int &i, int &j) {
         if constexpr (T::MMA) {
@@ -194,16 +204,24 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
     __syncthreads();
     if (total == 0) return;
     double ra[AL], rb[BL];
-    /* fetch position (tile origin and k offset), advanced incrementally */
-    int fm0 = 0, fn0 = 0, fk0 = 0;
-    auto advance = [&](int &m0, int &n0, int &k0) {
+    /* fetch position (tile index, tile origin and k offset), advanced
+     * incrementally over this CTA's share of the tiles */
+    int fti = PART ? pt.r : 0, fk0 = 0;
+    int fm0 = PART ? (pt.r % tm) * BM : 0, fn0 = PART ? (pt.r / tm) * BN : 0;
+    auto advance = [&](int &ti, int &m0, int &n0, int &k0) {
         k0 += BK;
         if (k0 >= nk * BK) {
             k0 = 0;
-            m0 += BM;
-            if (m0 >= tm * BM) {
-                m0 = 0;
-                n0 += BN;
+            if constexpr (PART) {
+                ti += pt.c;
+                m0 = (ti % tm) * BM;
+                n0 = (ti / tm) * BN;
+            } else {
+                m0 += BM;
+                if (m0 >= tm * BM) {
+                    m0 = 0;
+                    n0 += BN;
+                }
             }
         }
     };
@@ -268,12 +286,12 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
     for (int r = 0; r < TM; ++r)
 #pragma unroll
         for (int c = 0; c < TN; ++c) acc[r][c] = 0.0;
-    if constexpr (RMW) fetch_c(0, 0);
+    if constexpr (RMW) fetch_c(fm0, fn0);
     fetch();
     put(0);
     __syncthreads();
-    int cm0 = 0, cn0 = 0, ck0 = 0;   /* position being multiplied */
-    advance(fm0, fn0, fk0);
+    int cti = fti, cm0 = fm0, cn0 = fn0, ck0 = 0;   /* position being multiplied */
+    advance(fti, fm0, fn0, fk0);
     for (int it = 0; it < total; ++it) {
         const int cur = it & 1;
         if (it + 1 < total) fetch();
@@ -345,8 +363,8 @@ __device__ void gemm_core(int M, int N, int K, LA la, LB lb, LC lc, ST st, doubl
                 }
         }
         if (it + 1 < total) put(cur ^ 1);
-        advance(cm0, cn0, ck0);
-        advance(fm0, fn0, fk0);
+        advance(cti, cm0, cn0, ck0);
+        advance(fti, fm0, fn0, fk0);
         __syncthreads();
     }
 }
@@ -360,12 +378,29 @@ __device__ __forceinline__ void gemm(int M, int N, int K, LA la, LB lb, ST st, d
         M, N, K, la, lb, [](int, int) { return 0.0; }, st, sm, sa, sb);
 }
 
+/* One CTA's share pt of gemm's output tiles. */
+template <class T, bool AMF, bool BKF, class LA, class LB, class ST>
+__device__ __forceinline__ void gemm_part(int M, int N, int K, LA la, LB lb, ST st, double *sm,
+                                          Part pt)
+{
+    gemm_core<T, AMF, BKF, false, true>(
+        M, N, K, la, lb, [](int, int) { return 0.0; }, st, sm, Ident(), Ident(), pt);
+}
+
 /* C(i,j) <- st(i, j, sum_k a b, C(i,j)) with C read through lc */
 template <class T, bool AMF, bool BKF, class LA, class LB, class LC, class ST>
 __device__ __forceinline__ void gemm_rmw(int M, int N, int K, LA la, LB lb, LC lc, ST st,
                                          double *sm)
 {
     gemm_core<T, AMF, BKF, true>(M, N, K, la, lb, lc, st, sm);
+}
+
+/* One CTA's share pt of gemm_rmw's output tiles. */
+template <class T, bool AMF, bool BKF, class LA, class LB, class LC, class ST>
+__device__ __forceinline__ void gemm_rmw_part(int M, int N, int K, LA la, LB lb, LC lc, ST st,
+                                              double *sm, Part pt)
+{
+    gemm_core<T, AMF, BKF, true, true>(M, N, K, la, lb, lc, st, sm, Ident(), Ident(), pt);
 }
 
 /* Square-product dispatch by size: small lattices use 32x32 tiles. */
@@ -401,6 +436,54 @@ __device__ __forceinline__ void gemm_nn_rmw(int M, int N, int K, const double *A
     gemm_rmw<TSquare, true, true>(
         M, N, K, [=](int i, int k) { return A[i + (size_t)k * lda]; },
         [=](int k, int j) { return B[k + (size_t)j * ldb]; }, lc, st, sm);
+}
+
+/* A CTA's share of C = sum_k la lb (epilogue st) among pt.c > 1 CTAs, the
+ * tiles of the kind gemm_sq uses (SIMT for <= 32 x 32, else DMMA): among
+ * the DMMA shapes the one whose slowest share is cheapest (128 x 128 tiles
+ * issue about 1.5x the rate of 64 x 64 ones).  Every DMMA shape runs the
+ * same k sequence, so the result does not depend on the choice. */
+template <bool AMF, bool BKF, class LA, class LB, class ST>
+__device__ __forceinline__ void gemm_sq_part(int M, int N, int K, LA la, LB lb, ST st,
+                                             double *sm, Part pt)
+{
+    if (M <= 32 && N <= 32) {
+        gemm_part<TSm, AMF, BKF>(M, N, K, la, lb, st, sm, pt);
+        return;
+    }
+    const int w1 = ((M + 127) / 128 * ((N + 127) / 128) + pt.c - 1) / pt.c;
+    const int w2 = ((M + 63) / 64 * ((N + 63) / 64) + pt.c - 1) / pt.c;
+    if (M > 64 && N > 64 && 8 * w1 <= 3 * w2)
+        gemm_part<TSquareNR, AMF, BKF>(M, N, K, la, lb, st, sm, pt);
+    else
+        gemm_part<TMma, AMF, BKF>(M, N, K, la, lb, st, sm, pt);
+}
+
+/* A CTA's share of C = A B (column-major A, B), as gemm_nn. */
+template <class ST>
+__device__ __forceinline__ void gemm_nn_part(int M, int N, int K, const double *A, int lda,
+                                             const double *B, int ldb, ST st, double *sm,
+                                             Part pt)
+{
+    gemm_sq_part<true, true>(
+        M, N, K, [=](int i, int k) { return A[i + (size_t)k * lda]; },
+        [=](int k, int j) { return B[k + (size_t)j * ldb]; }, st, sm, pt);
+}
+
+/* A CTA's share of the read-modify-write product (as gemm_nn_rmw). */
+template <class LC, class ST>
+__device__ __forceinline__ void gemm_nn_rmw_part(int M, int N, int K, const double *A, int lda,
+                                                 const double *B, int ldb, LC lc, ST st,
+                                                 double *sm, Part pt)
+{
+    auto la = [=](int i, int k) { return A[i + (size_t)k * lda]; };
+    auto lb = [=](int k, int j) { return B[k + (size_t)j * ldb]; };
+    const int w1 = ((M + 127) / 128 * ((N + 63) / 64) + pt.c - 1) / pt.c;
+    const int w2 = ((M + 63) / 64 * ((N + 63) / 64) + pt.c - 1) / pt.c;
+    if (20 * w1 <= 13 * w2)
+        gemm_rmw_part<TSquare, true, true>(M, N, K, la, lb, lc, st, sm, pt);
+    else
+        gemm_rmw_part<TMma, true, true>(M, N, K, la, lb, lc, st, sm, pt);
 }
 
 /* ------------------------------------------------------------ workspace */
@@ -484,6 +567,11 @@ struct Smem {
     double *g0, *gt, *gam, *xs, *colA;
     QrSm q;          /* shared-memory QR view (overlaps gsm + phase) */
     void *spl;       /* split-GEMM context (mixed precision), else null   */
+    /* cluster cooperation: this CTA's rank among the CTAs that advance the
+     * chain together ({0, 1}: one CTA per chain) and the chain's command
+     * block through which rank 0 hands the others a product */
+    Part cl;
+    DqmcClCmd *cmd;
 };
 
 __host__ __device__ inline size_t smem_doubles(int n, int kb)
@@ -534,7 +622,138 @@ __device__ inline Smem carve(double *base, int n, int kb)
     q.rp = q.taus + 16;
     q.rf = q.rp + 16 * NW + NW + 8;
     s.spl = nullptr;
+    s.cl = Part();
+    s.cmd = nullptr;
     return s;
+}
+
+/* ------------------------------------------------- cluster cooperation */
+/* One chain advanced by the s.cl.c CTAs of a thread-block cluster: rank 0
+ * runs the sweep; at a product that splits by output tiles (the wrap, the
+ * B-block chain, the delayed-update G update) it writes a command into the
+ * chain's command block and every rank, rank 0 included, forms its share
+ * of the tiles.  The other ranks only ever wait at the cluster barrier for
+ * the next command (cl_serve); rank 0 ends every launch with CL_EXIT.
+ * Operands and results stay in global memory; the barrier's release /
+ * acquire at cluster scope orders them.  Every command runs the same
+ * barriers on every rank whatever its share, so the ranks cannot fall out
+ * of step. */
+enum {
+    CL_EXIT = 0,
+    CL_WRAP,        /* wrap_green                                      */
+    CL_WRAP_BACK,   /* wrap_green_back                                 */
+    CL_BBLOCK,      /* bblock                                          */
+    CL_GUPD,        /* delayed-update G update                         */
+    CL_QFORM,       /* qr_form_q_sm: column blocks                     */
+    CL_QT,          /* qr_apply_qt_sm: column blocks                   */
+    CL_QRIGHT,      /* qr_apply_right_sm: row blocks                   */
+    CL_TRSM,        /* trsm_upper: column ranges                       */
+    CL_UGEMM,       /* the UDV updates' products (udv_gemm kinds)      */
+    CL_ZY           /* flush_zy: row and column ranges                 */
+};
+
+__device__ __forceinline__ void cl_sync()
+{
+    asm volatile("barrier.cluster.arrive.release;\n\t"
+                 "barrier.cluster.wait.acquire;\n" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned cl_rank_hw()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ unsigned cl_size_hw()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
+/* Between two dependent steps of a split command: all ranks' shares. */
+__device__ __forceinline__ void part_sync(const Smem &s)
+{
+    if (s.cl.c > 1)
+        cl_sync();
+    else
+        __syncthreads();
+}
+
+/* Rank 0 hands a command to the cluster (no-op for one CTA per chain). */
+__device__ __forceinline__ void cl_post(const Smem &s, int op, const void *p0, const void *p1,
+                                        const void *p2, const void *p3, const void *p4,
+                                        const void *p5, int i0, int i1, int i2, double d0 = 0.0,
+                                        double d1 = 0.0, double d2 = 0.0, double d3 = 0.0)
+{
+    if (s.cl.c <= 1 || s.cl.r != 0) return;
+    if (threadIdx.x == 0) {
+        DqmcClCmd *c = s.cmd;
+        c->op = op;
+        c->i[0] = i0;
+        c->i[1] = i1;
+        c->i[2] = i2;
+        c->p[0] = p0;
+        c->p[1] = p1;
+        c->p[2] = p2;
+        c->p[3] = p3;
+        c->p[4] = p4;
+        c->p[5] = p5;
+        c->d[0] = d0;
+        c->d[1] = d1;
+        c->d[2] = d2;
+        c->d[3] = d3;
+    }
+    cl_sync();
+}
+
+/* End of a split command: every rank's share is in memory. */
+__device__ __forceinline__ void cl_done(const Smem &s)
+{
+    if (s.cl.c > 1) cl_sync();
+}
+
+/* Rank 0's copy of a shared-memory location of this CTA (every rank carves
+ * the same layout), read through distributed shared memory: the other
+ * ranks take the small per-call vectors (scalings, signs, the pivot order)
+ * that rank 0 holds in shared memory when a command starts. */
+__device__ __forceinline__ unsigned cl_rank0_addr(const void *p)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, 0;" : "=r"(r) : "r"(a));
+    return r;
+}
+
+/* Copies count doubles / ints at p from rank 0's shared memory into this
+ * CTA's (ranks > 0 only; rank 0 leaves them unchanged until the command's
+ * last barrier). */
+__device__ __forceinline__ void cl_pull(double *p, int count)
+{
+    for (int e = threadIdx.x; e < count; e += NT) {
+        double v;
+        asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(cl_rank0_addr(p + e))
+                     : "memory");
+        p[e] = v;
+    }
+}
+__device__ __forceinline__ void cl_pull(int *p, int count)
+{
+    for (int e = threadIdx.x; e < count; e += NT) {
+        int v;
+        asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(cl_rank0_addr(p + e))
+                     : "memory");
+        p[e] = v;
+    }
+}
+
+/* This rank's contiguous share [lo, hi) of count elementwise items. */
+__device__ __forceinline__ void part_range(const Smem &s, int count, int &lo, int &hi)
+{
+    const int per = (count + s.cl.c - 1) / s.cl.c;
+    lo = min(count, s.cl.r * per);
+    hi = min(count, lo + per);
 }
 
 /* Elementwise pass over e < count with U loads in flight per thread:
@@ -746,23 +965,30 @@ __device__ __noinline__ void qr_apply_qt_gm(int n, const double *A, const double
 }
 
 /* Solve R X = Y for the upper triangle R of A (ld n); X, Y n x n, X may not
- * alias Y.  Blocked by QNB rows from the bottom. */
+ * alias Y.  Blocked by QNB rows from the bottom.  Columns are independent:
+ * a split command (each rank of a cluster solves a range of columns). */
 __device__ __noinline__ void trsm_upper(int n, const double *A, const double *Y, double *X, Smem &s)
 {
+    cl_post(s, CL_TRSM, A, Y, X, nullptr, nullptr, nullptr, n, 0, 0);
+    int j0, j1;
+    part_range(s, n, j0, j1);
+    const int nj = j1 - j0;
+    const double *Yc = Y + (size_t)j0 * n;
+    double *Xc = X + (size_t)j0 * n;
     for (int i1 = n; i1 > 0; i1 -= QNB) {
         const int i0 = max(0, i1 - QNB), bs = i1 - i0;
         if (i1 < n) {
             gemm_rmw<TMmaWide, true, true>(
-                bs, n, n - i1,
+                bs, nj, n - i1,
                 [=](int i, int k) { return A[(i0 + i) + (size_t)(i1 + k) * n]; },
-                [=](int k, int j) { return X[(i1 + k) + (size_t)j * n]; },
-                [=](int i, int j) { return Y[(i0 + i) + (size_t)j * n]; },
-                [=](int i, int j, double v, double c) { X[(i0 + i) + (size_t)j * n] = c - v; },
+                [=](int k, int j) { return Xc[(i1 + k) + (size_t)j * n]; },
+                [=](int i, int j) { return Yc[(i0 + i) + (size_t)j * n]; },
+                [=](int i, int j, double v, double c) { Xc[(i0 + i) + (size_t)j * n] = c - v; },
                 s.gsm);
         } else {
-            for (int e = threadIdx.x; e < bs * n; e += NT) {
+            for (int e = threadIdx.x; e < bs * nj; e += NT) {
                 const int i = e % bs, j = e / bs;
-                X[(i0 + i) + (size_t)j * n] = Y[(i0 + i) + (size_t)j * n];
+                Xc[(i0 + i) + (size_t)j * n] = Yc[(i0 + i) + (size_t)j * n];
             }
         }
         double *Rb = s.phase;
@@ -771,10 +997,10 @@ __device__ __noinline__ void trsm_upper(int n, const double *A, const double *Y,
             Rb[e] = (i < bs && k < bs) ? A[(i0 + i) + (size_t)(i0 + k) * n] : 0.0;
         }
         __syncthreads();
-        for (int j = threadIdx.x; j < n; j += NT) {
+        for (int j = threadIdx.x; j < nj; j += NT) {
             double x[QNB];
 #pragma unroll
-            for (int i = 0; i < QNB; ++i) x[i] = (i < bs) ? X[(i0 + i) + (size_t)j * n] : 0.0;
+            for (int i = 0; i < QNB; ++i) x[i] = (i < bs) ? Xc[(i0 + i) + (size_t)j * n] : 0.0;
 #pragma unroll
             for (int i = QNB - 1; i >= 0; --i) {
                 if (i < bs) {
@@ -786,10 +1012,11 @@ __device__ __noinline__ void trsm_upper(int n, const double *A, const double *Y,
             }
 #pragma unroll
             for (int i = 0; i < QNB; ++i)
-                if (i < bs) X[(i0 + i) + (size_t)j * n] = x[i];
+                if (i < bs) Xc[(i0 + i) + (size_t)j * n] = x[i];
         }
         __syncthreads();
     }
+    cl_done(s);
 }
 
 /* ------------------------------------------------- pre-pivoted factor */
@@ -1347,13 +1574,15 @@ __device__ __noinline__ int qr_factor_sm(int n, double *A, double *tw, Smem &s, 
 }
 
 /* Q = H_1 ... H_n (n x n, ld n), column block by column block; panels
- * that start below a block's last column leave it unchanged. */
+ * that start below a block's last column leave it unchanged.  A split
+ * command (the ranks of a cluster take every c-th block). */
 __device__ __noinline__ void qr_form_q_sm(int n, const double *A, const double *tw, double *Q,
                                           Smem &s)
 {
+    cl_post(s, CL_QFORM, A, tw, Q, nullptr, nullptr, nullptr, n, 0, 0);
     QrSm &q = s.q;
     const int ld = q.ld, cb = q.cb, R = (n + 15) & ~15;
-    for (int jb = 0; jb < n; jb += cb) {
+    for (int jb = s.cl.r * cb; jb < n; jb += s.cl.c * cb) {
         const int nc = min(cb, n - jb);
         for (int c = 0; c < cb; ++c)
             for (int r = threadIdx.x; r < R; r += NT)
@@ -1364,36 +1593,49 @@ __device__ __noinline__ void qr_form_q_sm(int n, const double *A, const double *
                   [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nc, false); });
         qr_store_cols(q, n, Q, jb, nc);
     }
+    cl_done(s);
 }
 
-/* Y (n x ncols, ld n) <- Q^T Y. */
+/* Y (n x ncols, ld n) <- Q^T Y.  A split command (column blocks). */
 __device__ __noinline__ void qr_apply_qt_sm(int n, const double *A, const double *tw, double *Y,
                                             int ncols, Smem &s)
 {
+    cl_post(s, CL_QT, A, tw, Y, nullptr, nullptr, nullptr, n, ncols, 0);
     QrSm &q = s.q;
-    for (int jb = 0; jb < ncols; jb += q.cb) {
+    for (int jb = s.cl.r * q.cb; jb < ncols; jb += s.cl.c * q.cb) {
         const int nc = min(q.cb, ncols - jb);
         qr_load_cols(q, n, Y, jb, nc);
         qr_panels(q, n, A, tw, 0, 16, (n + 15) / 16,
                   [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nc, true); });
         qr_store_cols(q, n, Y, jb, nc);
     }
+    cl_done(s);
 }
 
 /* Xout = Xin Q diag(cs) (n x n, ld n; Xout may be Xin), a block of rows
- * at a time as (Xin Q)^T = Q^T Xin^T. */
+ * at a time as (Xin Q)^T = Q^T Xin^T.  A split command (row blocks) when cs
+ * is the signs vector s.vC, which the other ranks take from rank 0. */
 __device__ __noinline__ void qr_apply_right_sm(int n, const double *A, const double *tw,
                                                const double *Xin, double *Xout,
                                                const double *cs, Smem &s)
 {
     QrSm &q = s.q;
-    for (int r0 = 0; r0 < n; r0 += q.cb) {
+    const Part pt = cs == s.vC ? s.cl : Part();
+    if (pt.c > 1) {
+        cl_post(s, CL_QRIGHT, A, tw, Xin, Xout, nullptr, nullptr, n, 0, 0);
+        if (pt.r > 0) {
+            cl_pull(s.vC, n);
+            __syncthreads();
+        }
+    }
+    for (int r0 = pt.r * q.cb; r0 < n; r0 += pt.c * q.cb) {
         const int nr = min(q.cb, n - r0);
         qr_load_rows_t(q, n, Xin, r0, nr);
         qr_panels(q, n, A, tw, 0, 16, (n + 15) / 16,
                   [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nr, true); });
         qr_store_rows_t(q, n, Xout, r0, nr, cs);
     }
+    if (pt.c > 1) cl_done(s);
 }
 
 /* Dispatch: shared-memory QR when the block fits, else the global one. */
@@ -1469,6 +1711,58 @@ struct Scr {
     double *m0, *m1, *m2, *tw;
 };
 
+/* The UDV updates' n x n products as split commands of a cluster per
+ * chain (each rank forms a share of the output tiles; the small vectors the
+ * epilogues read come from rank 0's shared memory):
+ *   UG_LMUL1  C = (A B) diag(vA)            udv_lmul's B U D
+ *   UG_RMUL1  C = diag(vA) (A B)            udv_rmul's D T B
+ *   UG_COMB1  C = diag(vA) (A B) diag(vD)   udv_combine's D_L T_L U_R D_R
+ *   UG_RT     C = diag(1/vD) triu(A) B[perm, :]   R T_old of lmul / combine
+ * with the epilogue expressions of the one-CTA code, so the results are the
+ * same to the bit. */
+enum { UG_LMUL1 = 0, UG_RMUL1, UG_COMB1, UG_RT };
+
+__device__ __noinline__ void udv_gemm(int kind, int n, const double *A, const double *B,
+                                      double *C, Smem &s)
+{
+    cl_post(s, CL_UGEMM, A, B, C, nullptr, nullptr, nullptr, n, kind, 0);
+    if (s.cl.r > 0) {
+        if (kind == UG_RT) {
+            cl_pull(s.vD, n);
+            cl_pull(s.perm, n);
+        } else {
+            cl_pull(s.vA, n);
+            if (kind == UG_COMB1) cl_pull(s.vD, n);
+        }
+    }
+    const double *va = s.vA, *vd = s.vD;
+    const int *perm = s.perm;
+    switch (kind) {
+    case UG_LMUL1:
+        gemm_nn_part(n, n, n, A, n, B, n,
+                     [=](int i, int j, double v) { C[i + (size_t)j * n] = v * va[j]; }, s.gsm,
+                     s.cl);
+        break;
+    case UG_RMUL1:
+        gemm_nn_part(n, n, n, A, n, B, n,
+                     [=](int i, int j, double v) { C[i + (size_t)j * n] = va[i] * v; }, s.gsm,
+                     s.cl);
+        break;
+    case UG_COMB1:
+        gemm_nn_part(n, n, n, A, n, B, n,
+                     [=](int i, int j, double v) { C[i + (size_t)j * n] = va[i] * v * vd[j]; },
+                     s.gsm, s.cl);
+        break;
+    default:
+        gemm_sq_part<true, true>(
+            n, n, n, [=](int i, int k) { return k >= i ? A[i + (size_t)k * n] : 0.0; },
+            [=](int k, int j) { return B[perm[k] + (size_t)j * n]; },
+            [=](int i, int j, double v) { C[i + (size_t)j * n] = v / vd[i]; }, s.gsm, s.cl);
+        break;
+    }
+    cl_done(s);
+}
+
 /* u <- Bop * u where Bop = B (if B != nullptr) or expK * diag(v_l) for the
  * field row fl (single slice).  udv_lmul_impl, linalg.c:515-642, with
  * pre-pivoting and positive D (signs folded into U). */
@@ -1484,7 +1778,9 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
     const double *U = u.U;
     double *eD = s.vA, *vl = s.vD;
     double *M = w.m0;
-    if (B != nullptr) {
+    if (B != nullptr && s.cl.c > 1) {
+        udv_gemm(UG_LMUL1, n, B, U, M, s);
+    } else if (B != nullptr) {
         gemm_nn(n, n, n, B, n, U, n,
                 [=](int i, int j, double v) { M[i + (size_t)j * n] = v * eD[j]; }, s.gsm);
     } else {
@@ -1504,10 +1800,13 @@ __device__ __noinline__ void udv_lmul(int n, Udv u, const double *B, const doubl
     double *rd = s.vD;
     for (int i = threadIdx.x; i < n; i += NT) rd[i] = R[i + (size_t)i * n];
     __syncthreads();
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
-        [=](int k, int j) { return T[perm[k] + (size_t)j * n]; },
-        [=](int i, int j, double v) { Tn[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
+    if (s.cl.c > 1)
+        udv_gemm(UG_RT, n, R, T, Tn, s);
+    else
+        gemm_sq<true, true>(
+            n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
+            [=](int k, int j) { return T[perm[k] + (size_t)j * n]; },
+            [=](int i, int j, double v) { Tn[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
     {
         double *uT = u.T;
         const double *tn = Tn;
@@ -1533,8 +1832,11 @@ __device__ __noinline__ void udv_rmul(int n, Udv u, const double *B, Scr w, Smem
     const double *T = u.T;
     const double *eD = s.vA;
     double *M = w.m0;
-    gemm_nn(n, n, n, T, n, B, n,
-            [=](int i, int j, double v) { M[i + (size_t)j * n] = eD[i] * v; }, s.gsm);
+    if (s.cl.c > 1)
+        udv_gemm(UG_RMUL1, n, T, B, M, s);
+    else
+        gemm_nn(n, n, n, T, n, B, n,
+                [=](int i, int j, double v) { M[i + (size_t)j * n] = eD[i] * v; }, s.gsm);
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
     const int sg = qr_diag(n, w.m1, s, flag);
@@ -1588,9 +1890,12 @@ __device__ __noinline__ void udv_combine(int n, Udv l, Udv r, Udv o, Scr w, Smem
     double *M = w.m0;
     {
         const double *eR = s.vD;
-        gemm_nn(n, n, n, TL, n, UR, n,
-                [=](int i, int j, double v) { M[i + (size_t)j * n] = eL[i] * v * eR[j]; },
-                s.gsm);
+        if (s.cl.c > 1)
+            udv_gemm(UG_COMB1, n, TL, UR, M, s);
+        else
+            gemm_nn(n, n, n, TL, n, UR, n,
+                    [=](int i, int j, double v) { M[i + (size_t)j * n] = eL[i] * v * eR[j]; },
+                    s.gsm);
     }
     prepivot(n, M, w.m1, s, flag);
     const int nt = qr_factor(n, w.m1, w.tw, s, flag);
@@ -1612,10 +1917,13 @@ __device__ __noinline__ void udv_combine(int n, Udv l, Udv r, Udv o, Scr w, Smem
     double *rd = s.vD;
     for (int i = threadIdx.x; i < n; i += NT) rd[i] = R[i + (size_t)i * n];
     __syncthreads();
-    gemm_sq<true, true>(
-        n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
-        [=](int k, int j) { return TR[perm[k] + (size_t)j * n]; },
-        [=](int i, int j, double v) { To[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
+    if (s.cl.c > 1)
+        udv_gemm(UG_RT, n, R, TR, To, s);
+    else
+        gemm_sq<true, true>(
+            n, n, n, [=](int i, int k) { return k >= i ? R[i + (size_t)k * n] : 0.0; },
+            [=](int k, int j) { return TR[perm[k] + (size_t)j * n]; },
+            [=](int i, int j, double v) { To[i + (size_t)j * n] = v / rd[i]; }, s.gsm);
     for (int i = threadIdx.x; i < n; i += NT) o.ell[i] = s.vB[i];
     if (threadIdx.x == 0) *o.det = *l.det * ((nt & 1) ? -1.0 : 1.0) * sg;
     __syncthreads();
@@ -1792,10 +2100,106 @@ __device__ __noinline__ int udv_green2(int n, Udv l, Udv r, double *G, double *X
 
 /* ----------------------------------------------------- slice operations */
 /* G <- B_l G B_l^{-1} = expK diag(v) G diag(1/v) expKinv (green.c:509-527). */
+/* The wrap and the B-block chain as split commands of a cluster per chain:
+ * rank 0 posts them (cl_post) and every rank forms its share of the
+ * elementwise pass and of each product's tiles, with a cluster barrier
+ * between dependent steps.  Same arithmetic per element as wrap_green,
+ * wrap_green_back and bblock below. */
+__device__ __noinline__ void wrap_green_cl(int n, double *G, double *tmp, const double *expK,
+                           const double *expKinv, const signed char *fl, double v0,
+                           double v1, double vi0, double vi1, Smem &s)
+{
+    cl_post(s, CL_WRAP, G, tmp, expK, expKinv, fl, nullptr, n, 0, 0, v0, v1, vi0, vi1);
+    double *vv = s.vA, *vi = s.vB;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        const bool up = fl[k] > 0;
+        vv[k] = up ? v1 : v0;
+        vi[k] = up ? vi1 : vi0;
+    }
+    __syncthreads();
+    /* G <- diag(v) G diag(1/v) in place (G is overwritten below), so both
+     * products are plain */
+    int lo, hi;
+    part_range(s, n * n, lo, hi);
+    ew_batched(hi - lo, [=](int e) { return G[lo + e]; }, [=](int e, double x) {
+        const int f = lo + e;
+        G[f] = x * (vv[f % n] * vi[f / n]);
+    });
+    part_sync(s);
+    gemm_nn_part(n, n, n, expK, n, G, n,
+                 [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; }, s.gsm, s.cl);
+    part_sync(s);
+    gemm_nn_part(n, n, n, tmp, n, expKinv, n,
+                 [=](int i, int j, double v) { G[i + (size_t)j * n] = v; }, s.gsm, s.cl);
+    cl_done(s);
+}
+
+__device__ __noinline__ void wrap_green_back_cl(int n, double *G, double *tmp, const double *expK,
+                                             const double *expKinv, const signed char *fl,
+                                             double v0, double v1, double vi0, double vi1,
+                                             Smem &s)
+{
+    cl_post(s, CL_WRAP_BACK, G, tmp, expK, expKinv, fl, nullptr, n, 0, 0, v0, v1, vi0, vi1);
+    double *vv = s.vA, *vi = s.vB;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        const bool up = fl[k] > 0;
+        vv[k] = up ? v1 : v0;
+        vi[k] = up ? vi1 : vi0;
+    }
+    gemm_nn_part(n, n, n, expKinv, n, G, n,
+                 [=](int i, int j, double v) { tmp[i + (size_t)j * n] = v; }, s.gsm, s.cl);
+    part_sync(s);
+    gemm_nn_part(n, n, n, tmp, n, expK, n,
+                 [=](int i, int j, double v) { G[i + (size_t)j * n] = (vi[i] * v) * vv[j]; },
+                 s.gsm, s.cl);
+    cl_done(s);
+}
+
+__device__ __noinline__ void bblock_cl(int n, int l0, int len, const signed char *field, const double *expK,
+                       double v0, double v1, double *out, double *X, double *Y, Smem &s)
+{
+    cl_post(s, CL_BBLOCK, field, expK, out, X, Y, nullptr, n, l0, len, v0, v1);
+    /* Intermediate products are stored row-scaled by the next slice's
+     * diag(v) (folded into the producing GEMM's epilogue), so every
+     * product is a plain expK * X. */
+    const signed char *f0 = field + (size_t)l0 * n;
+    double *first = (len == 1) ? out : X;
+    double *vv = s.vA;
+    for (int i = threadIdx.x; i < n; i += NT)
+        vv[i] = (len == 1) ? 1.0 : (field[(size_t)(l0 + 1) * n + i] > 0 ? v1 : v0);
+    __syncthreads();
+    int lo, hi;
+    part_range(s, n * n, lo, hi);
+    ew_batched(hi - lo, [=](int e) { return expK[lo + e]; }, [=](int e, double x) {
+        const int f = lo + e;
+        first[f] = vv[f % n] * (x * (f0[f / n] > 0 ? v1 : v0));
+    });
+    part_sync(s);
+    const double *src = first;
+    for (int p = 1; p < len; ++p) {
+        const bool lastp = (p == len - 1);
+        double *dst = lastp ? out : ((src == X) ? Y : X);
+        if (!lastp) {
+            const signed char *fn = field + (size_t)(l0 + p + 1) * n;
+            for (int i = threadIdx.x; i < n; i += NT) vv[i] = fn[i] > 0 ? v1 : v0;
+        }
+        gemm_nn_part(n, n, n, expK, n, src, n,
+                     [=](int i, int j, double v) { dst[i + (size_t)j * n] = lastp ? v : vv[i] * v; },
+                     s.gsm, s.cl);
+        if (!lastp) part_sync(s);
+        src = dst;
+    }
+    cl_done(s);
+}
+
 __device__ __noinline__ void wrap_green(int n, double *G, double *tmp, const double *expK,
                            const double *expKinv, const signed char *fl, double v0,
                            double v1, double vi0, double vi1, Smem &s)
 {
+    if (s.cl.c > 1) {
+        wrap_green_cl(n, G, tmp, expK, expKinv, fl, v0, v1, vi0, vi1, s);
+        return;
+    }
     double *vv = s.vA, *vi = s.vB;
     for (int k = threadIdx.x; k < n; k += NT) {
         const bool up = fl[k] > 0;
@@ -1820,6 +2224,10 @@ __device__ __noinline__ void wrap_green_back(int n, double *G, double *tmp, cons
                                              double v0, double v1, double vi0, double vi1,
                                              Smem &s)
 {
+    if (s.cl.c > 1) {
+        wrap_green_back_cl(n, G, tmp, expK, expKinv, fl, v0, v1, vi0, vi1, s);
+        return;
+    }
     double *vv = s.vA, *vi = s.vB;
     for (int k = threadIdx.x; k < n; k += NT) {
         const bool up = fl[k] > 0;
@@ -1836,6 +2244,10 @@ __device__ __noinline__ void wrap_green_back(int n, double *G, double *tmp, cons
 __device__ __noinline__ void bblock(int n, int l0, int len, const signed char *field, const double *expK,
                        double v0, double v1, double *out, double *X, double *Y, Smem &s)
 {
+    if (s.cl.c > 1) {
+        bblock_cl(n, l0, len, field, expK, v0, v1, out, X, Y, s);
+        return;
+    }
     /* Intermediate products are stored row-scaled by the next slice's
      * diag(v) (folded into the producing GEMM's epilogue), so every
      * product is a plain expK * X. */

@@ -244,6 +244,7 @@ struct dqmc_engine {
     int nbin = 0;
     size_t smem = 0, msmem = 0, smem2 = 0;
     int per_sm = 1;           /* CTAs per SM of the sweep kernels (1 or 2) */
+    int cl = 1;               /* CTAs per chain of the sweep kernel (a cluster) */
     bool prepared = false;
     /* per-launch CUDA events (kind 0 = sweep kernel, 1 = measurement) */
     bool timing = false;
@@ -328,6 +329,18 @@ dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
     }
     if (d.precision != DQMC_PREC_FP64 && d.precision != DQMC_PREC_MIXED) {
         set_err("precision %d is neither DQMC_PREC_FP64 nor DQMC_PREC_MIXED", d.precision);
+        return nullptr;
+    }
+    if (d.chain_ctas < 0 || d.chain_ctas > DQMC_MAX_CHAIN_CTAS) {
+        set_err("chain_ctas %d is outside 0..%d", d.chain_ctas, DQMC_MAX_CHAIN_CTAS);
+        return nullptr;
+    }
+    if (d.chain_ctas > 1 && d.precision == DQMC_PREC_MIXED) {
+        set_err("chain_ctas %d: a cluster per chain runs the FP64 products only", d.chain_ctas);
+        return nullptr;
+    }
+    if (d.chain_ctas > 1 && d.ctas_per_sm == 2) {
+        set_err("chain_ctas %d needs one CTA per SM (ctas_per_sm 0 or 1)", d.chain_ctas);
         return nullptr;
     }
     if (cudaSetDevice(d.device) != cudaSuccess) {
@@ -794,8 +807,9 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
     /* Two chains per SM when the batch has more chains than SMs and two
      * CTAs fit in shared memory: the second chain fills the first one's
      * barrier and reduction latency. */
+    int nsm = 148;
     {
-        int dev = 0, nsm = 148;
+        int dev = 0;
         CU(cudaGetDevice(&dev));
         CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         const bool fits2 = 2 * (e->smem2 + 1024) <= 228 * 1024;
@@ -804,9 +818,40 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
          * registers: one CTA per SM */
         bool two = false;
         for (const HChain &c : e->chains) two = two || !e->models[c.model].ph;
-        e->per_sm =
-            (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 && !mixed && !two ? 2 : 1;
+        e->per_sm = (want == 2 || (want == 0 && (int)nc > nsm)) && fits2 && !mixed && !two &&
+                            e->desc.chain_ctas <= 1
+                        ? 2
+                        : 1;
         if (e->per_sm == 2) CU(dq2x::set_attrs(e->smem2, e->msmem));
+    }
+    /* One thread-block cluster per chain.  Automatic (chain_ctas = 0) for
+     * FP64 batches of fewer chains than SMs whose largest lattice has
+     * n >= 128 (below that the split products are too small to pay): the
+     * largest cluster such that every chain's cluster is resident at once
+     * (a second wave of clusters costs more than narrower clusters). */
+    e->cl = 1;
+    if (e->desc.chain_ctas == 0 && !mixed && e->per_sm == 1 && maxn >= 128) {
+        static const int sizes[] = {16, 12, 8, 6, 4, 3, 2};
+        for (int cc : sizes) {
+            if ((long)nc * cc > nsm) continue;
+            int fit = 0;
+            if (dq::cluster_fit(cc, e->smem, &fit) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if (fit >= (int)nc) {
+                e->cl = cc;
+                break;
+            }
+        }
+    } else if (e->desc.chain_ctas > 1) {
+        int fit = 0;
+        CU(dq::cluster_fit(e->desc.chain_ctas, e->smem, &fit));
+        if (fit < 1)
+            return set_err("dqmc_engine_prepare: a cluster of %d CTAs with %zu B of shared "
+                           "memory each cannot be resident on this device",
+                           e->desc.chain_ctas, e->smem);
+        e->cl = e->desc.chain_ctas;
     }
     dq::k_init<<<(unsigned)nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels);
     CU(cudaGetLastError());
@@ -863,7 +908,10 @@ int dqmc_sweep(dqmc_engine *e, int nsweeps)
     const int per = e->desc.udv_diag ? 1 : nsweeps;
     for (int done = 0; done < nsweeps; done += per) {
         ev_begin(e, 0);
-        if (e->per_sm == 2)
+        if (e->cl > 1)
+            CU(dq::launch_sweep_cluster(nc, e->cl, e->smem, e->stream, e->dchains, e->dmodels,
+                                        kflags(e), per, e->dorder));
+        else if (e->per_sm == 2)
             dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), per,
                                  e->dorder);
         else
@@ -942,7 +990,10 @@ int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
     for (int s = 0; s < nsweeps; ++s) {
         const int f = kflags(e) | dq::KF_MEASURE;
         ev_begin(e, 0);
-        if (e->per_sm == 2)
+        if (e->cl > 1)
+            CU(dq::launch_sweep_cluster(nc, e->cl, e->smem, e->stream, e->dchains, e->dmodels, f,
+                                        1, e->dorder));
+        else if (e->per_sm == 2)
             dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, f, 1, e->dorder);
         else
             dq::launch_sweep(nc, e->smem, e->stream, e->dchains, e->dmodels, f, 1, e->dorder);
@@ -1018,6 +1069,14 @@ int dqmc_synchronize(dqmc_engine *e)
 }
 
 int dqmc_chain_count(const dqmc_engine *e) { return e ? (int)e->chains.size() : 0; }
+
+int dqmc_engine_residency(const dqmc_engine *e, int *ctas_per_sm, int *chain_ctas)
+{
+    if (!e || !e->prepared) return set_err("dqmc_engine_residency: engine not prepared");
+    if (ctas_per_sm) *ctas_per_sm = e->per_sm;
+    if (chain_ctas) *chain_ctas = e->cl;
+    return 0;
+}
 
 int dqmc_chain_dims(const dqmc_engine *e, int chain, int *n, int *L)
 {

@@ -58,12 +58,187 @@ __device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
  * Zs and Ys are formed one row / one column per thread (FP64 FMAs on the
  * accepted columns / rows of G, coalesced across the CTA): no CTA-wide GEMM
  * pipeline for these thin products. */
+/* Zs_B rows and Ys_B columns of a site block's flush (block_flush, after
+ * the inverses): TuP, facs and the pair-staging operands TvP, Qa, PaT (in
+ * the GEMM staging area) and the accepted list are in shared memory.  Rows
+ * and columns are independent: a split command of a cluster per chain,
+ * whose other ranks take those small operands from rank 0's shared memory
+ * and form a contiguous range of rows and columns each. */
+__device__ __noinline__ void flush_zy(int n, int i0, int m, int mA, const double *G, double *Zs,
+                                      double *Ys, int ldy, const double *TuP,
+                                      const double *facs, Smem &s)
+{
+    constexpr int KB = DQMC_MAX_KB;
+    constexpr int LT = KB + 2;
+    const int tid = threadIdx.x;
+    cl_post(s, CL_ZY, G, Zs, Ys, TuP, facs, nullptr, n, i0, m | (mA << 8) | (ldy << 16));
+    double *TvP = s.gsm + 2 * KB * LT, *YA = s.gsm + KB * LT, *ZA = s.gsm;
+    const int *alist = s.iscr;
+    if (s.cl.r > 0) {
+        cl_pull(const_cast<double *>(TuP), KB * LT);
+        cl_pull(TvP, KB * LT);
+        cl_pull(const_cast<double *>(facs), KB);
+        cl_pull(s.iscr, KB);
+        if (mA > 0) {
+            cl_pull(YA, KB * LT);
+            cl_pull(ZA, KB * LT);
+        }
+        __syncthreads();
+    }
+    int lo, hi;
+    part_range(s, n, lo, hi);
+    /* Zs_B rows and Ys_B columns, after the mA staged ones.  Pass 1: the
+     * G part, (E_B - G[:,B]) Tu and Tv^T G[B,:]; pass 2 (staged block):
+     * + Zs_A Qa and - Pa Ys_A, the staged operands of a row / column loaded
+     * as one batch; F scales Zs_B once, at the end. */
+    const double *Qa = YA, *PaT = ZA;
+    double *ZsB = Zs + (size_t)mA * n;
+    double *YsB = Ys + mA;
+    const bool two = mA > 0;
+    for (int i = lo + tid; i < hi; i += NT) {
+        double x[KB];
+#pragma unroll
+        for (int q = 0; q < KB; ++q) {
+            const int c = i0 + alist[q];
+            x[q] = q < m ? (i == c ? 1.0 : 0.0) - G[i + (size_t)c * n] : 0.0;
+        }
+        for (int p0 = 0; p0 < m; p0 += 8) {
+            double z[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) z[u] = 0.0;
+#pragma unroll
+            for (int q0 = 0; q0 < KB; q0 += 8) {
+                if (q0 < m) {
+#pragma unroll
+                    for (int q = q0; q < q0 + 8; ++q) {
+#pragma unroll
+                        for (int u = 0; u < 8; u += 2) {
+                            const double2 t =
+                                *reinterpret_cast<const double2 *>(TuP + q * LT + p0 + u);
+                            z[u] = fma(x[q], t.x, z[u]);
+                            z[u + 1] = fma(x[q], t.y, z[u + 1]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = two ? z[u] : z[u] * facs[p0 + u];
+        }
+    }
+    for (int j = lo + tid; j < hi; j += NT) {
+        double y[KB];
+#pragma unroll
+        for (int q = 0; q < KB; ++q)
+            y[q] = q < m ? G[(i0 + alist[q]) + (size_t)j * n] : 0.0;
+        for (int p0 = 0; p0 < m; p0 += 8) {
+            double z[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) z[u] = 0.0;
+#pragma unroll
+            for (int q0 = 0; q0 < KB; q0 += 8) {
+                if (q0 < m) {
+#pragma unroll
+                    for (int q = q0; q < q0 + 8; ++q) {
+#pragma unroll
+                        for (int u = 0; u < 8; u += 2) {
+                            const double2 t =
+                                *reinterpret_cast<const double2 *>(TvP + q * LT + p0 + u);
+                            z[u] = fma(t.x, y[q], z[u]);
+                            z[u + 1] = fma(t.y, y[q], z[u + 1]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+        }
+    }
+    if (two) {
+        /* each thread re-reads only what it wrote in pass 1 */
+        for (int i = lo + tid; i < hi; i += NT) {
+            double za[KB];
+#pragma unroll
+            for (int k = 0; k < KB; ++k) za[k] = k < mA ? Zs[i + (size_t)k * n] : 0.0;
+            for (int p0 = 0; p0 < m; p0 += 8) {
+                double z[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    z[u] = p0 + u < m ? ZsB[i + (size_t)(p0 + u) * n] : 0.0;
+#pragma unroll
+                for (int k0 = 0; k0 < KB; k0 += 8) {
+                    if (k0 < mA) {
+#pragma unroll
+                        for (int k = k0; k < k0 + 8; ++k) {
+#pragma unroll
+                            for (int u = 0; u < 8; u += 2) {
+                                const double2 t =
+                                    *reinterpret_cast<const double2 *>(Qa + k * LT + p0 + u);
+                                z[u] = fma(za[k], t.x, z[u]);
+                                z[u + 1] = fma(za[k], t.y, z[u + 1]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = z[u] * facs[p0 + u];
+            }
+        }
+        for (int j = lo + tid; j < hi; j += NT) {
+            double ya[KB];
+#pragma unroll
+            for (int k = 0; k < KB; ++k) ya[k] = k < mA ? Ys[k + (size_t)j * ldy] : 0.0;
+            for (int p0 = 0; p0 < m; p0 += 8) {
+                double z[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    z[u] = p0 + u < m ? YsB[(p0 + u) + (size_t)j * ldy] : 0.0;
+#pragma unroll
+                for (int k0 = 0; k0 < KB; k0 += 8) {
+                    if (k0 < mA) {
+#pragma unroll
+                        for (int k = k0; k < k0 + 8; ++k) {
+#pragma unroll
+                            for (int u = 0; u < 8; u += 2) {
+                                const double2 t =
+                                    *reinterpret_cast<const double2 *>(PaT + k * LT + p0 + u);
+                                z[u] = fma(t.x, ya[k], z[u]);
+                                z[u + 1] = fma(t.y, ya[k], z[u + 1]);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+            }
+        }
+    }
+    if (s.cl.c > 1)
+        cl_done(s);
+    else
+        __syncthreads();
+}
+
 /* The flush of one spin's site block after the proposals: the inverses Tu,
  * Tv from the recorded rows / columns, Zs and Ys (with the staged block's
  * corrections when mA > 0), and the G update when `flush`.  Rrow, Ccol,
  * facs: that spin's records; TuP: where Tu is laid out with even rows (the
  * spin's own Rrow area, free once the inverses exist).  Returns the staged
  * count left for the next block (0 after a G update). */
+/* G -= Zs Ys as a split command of a cluster per chain (FP64). */
+__device__ __noinline__ void g_update_cl(int n, int mt, double *G, const double *Zs,
+                                         const double *Ys, int ldy, Smem &s)
+{
+    cl_post(s, CL_GUPD, G, Zs, Ys, nullptr, nullptr, nullptr, n, mt, ldy);
+    gemm_nn_rmw_part(
+        n, n, mt, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
+        [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm, s.cl);
+    cl_done(s);
+}
+
 /* G -= Zs Ys (rank mt): FP64 tiles, or the split product in mixed mode. */
 __device__ __forceinline__ void g_update(int n, int mt, double *G, const double *Zs,
                                          const double *Ys, int ldy, const DqmcChainDev *ch,
@@ -76,9 +251,69 @@ __device__ __forceinline__ void g_update(int n, int mt, double *G, const double 
     }
 #endif
     (void)ch;
+    if (s.cl.c > 1) {
+        g_update_cl(n, mt, G, Zs, Ys, ldy, s);
+        return;
+    }
     gemm_nn_rmw(
         n, n, mt, Zs, n, Ys, ldy, [=](int i, int j) { return G[i + (size_t)j * n]; },
         [=](int i, int j, double v, double c) { G[i + (size_t)j * n] = c - v; }, s.gsm);
+}
+
+/* Ranks 1.. of a chain's cluster: form this rank's share of each command
+ * rank 0 posts, until CL_EXIT.  The command block is read after the
+ * barrier that publishes it and before the command's own barriers, so
+ * rank 0 never rewrites it while it is being read. */
+__device__ __noinline__ void cl_serve(Smem &s)
+{
+    for (;;) {
+        cl_sync();
+        const DqmcClCmd *c = s.cmd;
+        const int op = c->op;
+        if (op == CL_EXIT) break;
+        const int i0 = c->i[0], i1 = c->i[1], i2 = c->i[2];
+        const void *p0 = c->p[0], *p1 = c->p[1], *p2 = c->p[2], *p3 = c->p[3], *p4 = c->p[4];
+        const double d0 = c->d[0], d1 = c->d[1], d2 = c->d[2], d3 = c->d[3];
+        switch (op) {
+        case CL_WRAP:
+            wrap_green_cl(i0, (double *)p0, (double *)p1, (const double *)p2,
+                          (const double *)p3, (const signed char *)p4, d0, d1, d2, d3, s);
+            break;
+        case CL_WRAP_BACK:
+            wrap_green_back_cl(i0, (double *)p0, (double *)p1, (const double *)p2,
+                               (const double *)p3, (const signed char *)p4, d0, d1, d2, d3, s);
+            break;
+        case CL_BBLOCK:
+            bblock_cl(i0, i1, i2, (const signed char *)p0, (const double *)p1, d0, d1,
+                      (double *)p2, (double *)p3, (double *)p4, s);
+            break;
+        case CL_GUPD:
+            g_update_cl(i0, i1, (double *)p0, (const double *)p1, (const double *)p2, i2, s);
+            break;
+        case CL_QFORM:
+            qr_form_q_sm(i0, (const double *)p0, (const double *)p1, (double *)p2, s);
+            break;
+        case CL_QT:
+            qr_apply_qt_sm(i0, (const double *)p0, (const double *)p1, (double *)p2, i1, s);
+            break;
+        case CL_QRIGHT:
+            qr_apply_right_sm(i0, (const double *)p0, (const double *)p1, (const double *)p2,
+                              (double *)p3, s.vC, s);
+            break;
+        case CL_TRSM:
+            trsm_upper(i0, (const double *)p0, (const double *)p1, (double *)p2, s);
+            break;
+        case CL_UGEMM:
+            udv_gemm(i1, i0, (const double *)p0, (const double *)p1, (double *)p2, s);
+            break;
+        case CL_ZY:
+            flush_zy(i0, i1, i2 & 255, (i2 >> 8) & 255, (const double *)p0, (double *)p1,
+                     (double *)p2, i2 >> 16, (const double *)p3, (const double *)p4, s);
+            break;
+        default:
+            break;
+        }
+    }
 }
 
 __device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G, double *Zs,
@@ -169,136 +404,7 @@ __device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G,
     }
     __syncthreads();
     pc.charge(ch, DQMC_PH_FLUSH);
-    /* Zs_B rows and Ys_B columns, after the mA staged ones.  Pass 1: the
-     * G part, (E_B - G[:,B]) Tu and Tv^T G[B,:]; pass 2 (staged block):
-     * + Zs_A Qa and - Pa Ys_A, the staged operands of a row / column loaded
-     * as one batch; F scales Zs_B once, at the end. */
-    const double *Qa = YA, *PaT = ZA;
-    double *ZsB = Zs + (size_t)mA * n;
-    double *YsB = Ys + mA;
-    const bool two = mA > 0;
-    for (int i = tid; i < n; i += NT) {
-        double x[KB];
-#pragma unroll
-        for (int q = 0; q < KB; ++q) {
-            const int c = i0 + alist[q];
-            x[q] = q < m ? (i == c ? 1.0 : 0.0) - G[i + (size_t)c * n] : 0.0;
-        }
-        for (int p0 = 0; p0 < m; p0 += 8) {
-            double z[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) z[u] = 0.0;
-#pragma unroll
-            for (int q0 = 0; q0 < KB; q0 += 8) {
-                if (q0 < m) {
-#pragma unroll
-                    for (int q = q0; q < q0 + 8; ++q) {
-#pragma unroll
-                        for (int u = 0; u < 8; u += 2) {
-                            const double2 t =
-                                *reinterpret_cast<const double2 *>(TuP + q * LT + p0 + u);
-                            z[u] = fma(x[q], t.x, z[u]);
-                            z[u + 1] = fma(x[q], t.y, z[u + 1]);
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = two ? z[u] : z[u] * facs[p0 + u];
-        }
-    }
-    for (int j = tid; j < n; j += NT) {
-        double y[KB];
-#pragma unroll
-        for (int q = 0; q < KB; ++q)
-            y[q] = q < m ? G[(i0 + alist[q]) + (size_t)j * n] : 0.0;
-        for (int p0 = 0; p0 < m; p0 += 8) {
-            double z[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) z[u] = 0.0;
-#pragma unroll
-            for (int q0 = 0; q0 < KB; q0 += 8) {
-                if (q0 < m) {
-#pragma unroll
-                    for (int q = q0; q < q0 + 8; ++q) {
-#pragma unroll
-                        for (int u = 0; u < 8; u += 2) {
-                            const double2 t =
-                                *reinterpret_cast<const double2 *>(TvP + q * LT + p0 + u);
-                            z[u] = fma(t.x, y[q], z[u]);
-                            z[u + 1] = fma(t.y, y[q], z[u + 1]);
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
-        }
-    }
-    if (two) {
-        /* each thread re-reads only what it wrote in pass 1 */
-        for (int i = tid; i < n; i += NT) {
-            double za[KB];
-#pragma unroll
-            for (int k = 0; k < KB; ++k) za[k] = k < mA ? Zs[i + (size_t)k * n] : 0.0;
-            for (int p0 = 0; p0 < m; p0 += 8) {
-                double z[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    z[u] = p0 + u < m ? ZsB[i + (size_t)(p0 + u) * n] : 0.0;
-#pragma unroll
-                for (int k0 = 0; k0 < KB; k0 += 8) {
-                    if (k0 < mA) {
-#pragma unroll
-                        for (int k = k0; k < k0 + 8; ++k) {
-#pragma unroll
-                            for (int u = 0; u < 8; u += 2) {
-                                const double2 t =
-                                    *reinterpret_cast<const double2 *>(Qa + k * LT + p0 + u);
-                                z[u] = fma(za[k], t.x, z[u]);
-                                z[u + 1] = fma(za[k], t.y, z[u + 1]);
-                            }
-                        }
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = z[u] * facs[p0 + u];
-            }
-        }
-        for (int j = tid; j < n; j += NT) {
-            double ya[KB];
-#pragma unroll
-            for (int k = 0; k < KB; ++k) ya[k] = k < mA ? Ys[k + (size_t)j * ldy] : 0.0;
-            for (int p0 = 0; p0 < m; p0 += 8) {
-                double z[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    z[u] = p0 + u < m ? YsB[(p0 + u) + (size_t)j * ldy] : 0.0;
-#pragma unroll
-                for (int k0 = 0; k0 < KB; k0 += 8) {
-                    if (k0 < mA) {
-#pragma unroll
-                        for (int k = k0; k < k0 + 8; ++k) {
-#pragma unroll
-                            for (int u = 0; u < 8; u += 2) {
-                                const double2 t =
-                                    *reinterpret_cast<const double2 *>(PaT + k * LT + p0 + u);
-                                z[u] = fma(t.x, ya[k], z[u]);
-                                z[u + 1] = fma(t.y, ya[k], z[u + 1]);
-                            }
-                        }
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
-            }
-        }
-    }
-    __syncthreads();
+    flush_zy(n, i0, m, mA, G, Zs, Ys, ldy, TuP, facs, s);
     const int mt = mA + m;
     if (!flush) {
         pc.charge(ch, DQMC_PH_FLUSH);
@@ -925,8 +1031,9 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     return rebuild(0, left, false, 0);
 }
 
-/* One CTA per chain; order[b] names the chain of block b (longest first,
- * so a batch of uneven chains does not end on a late-starting long one). */
+/* One CTA per chain, or one thread-block cluster per chain (cl_serve);
+ * order[b] names the chain of CTA (cluster) b, longest first, so a batch of
+ * uneven chains does not end on a late-starting long one. */
 __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps,
             const int *order)
@@ -935,65 +1042,80 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     __shared__ int flag;
     __shared__ uint64_t rng[4];
     __shared__ unsigned long long att, acc;
-    DqmcChainDev *ch = &chains[order ? order[blockIdx.x] : blockIdx.x];
+    /* a launch without clusters is a launch of one-CTA clusters */
+    const int cc = max(1, (int)cl_size_hw()), cr = cc > 1 ? (int)cl_rank_hw() : 0;
+    const int slot = (int)(blockIdx.x / (unsigned)cc);
+    DqmcChainDev *ch = &chains[order ? order[slot] : slot];
     const DqmcModelDev &md = models[ch->model];
+    Smem s = carve(smraw, ch->n, ch->kb);
+    s.cl = Part{cr, cc};
+    s.cmd = &ch->cl;
+    if (cr > 0) {
+        cl_serve(s);
+        return;
+    }
     if (threadIdx.x == 0) flag = ch->status;
     __syncthreads();
-    if (flag) return;
-    Smem s = carve(smraw, ch->n, ch->kb);
+    if (!flag) {
 #if DQMC_MINB == 1
-    __shared__ SplCtx spl;
-    if (kflags & KF_MIXED) {
-        spl_setup(&spl);
-        s.spl = &spl;
-    }
-#endif
-    for (int sw = 0; sw < nsweeps; ++sw) {
-        if (threadIdx.x == 0) {
-            for (int i = 0; i < 4; ++i) rng[i] = ch->rng[i];
-            att = 0;
-            acc = 0;
-            ch->meas_accepted = ch->accepted;
-            ch->meas_attempts = ch->attempts;
-        }
-        __syncthreads();
-        const bool back = ch->alt && ch->dir;
-        bool ok = back ? sweep_body_back(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr)
-                       : sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
-        __syncthreads();
-#if DQMC_MINB == 1
-        if (s.spl && spl.err) {   /* a split product was abandoned */
-            ok = false;
-            if (threadIdx.x == 0) flag |= DQMC_ST_TIMEOUT;
-            __syncthreads();
+        __shared__ SplCtx spl;
+        if ((kflags & KF_MIXED) && cc == 1) {
+            spl_setup(&spl);
+            s.spl = &spl;
         }
 #endif
-        if (threadIdx.x == 0) {
-            for (int i = 0; i < 4; ++i) ch->rng[i] = rng[i];
-            ch->attempts += att;
-            ch->accepted += acc;
-            if (ok && !flag) {
-                ch->sweeps++;
-                ch->bvalid = 1;
-                if (ch->alt) {   /* dqmc.c:806-810, 943-946 */
-                    ch->dir = back ? 0 : 1;
-                    ch->pvalid = back ? 0 : 1;
-                    ch->svalid = back ? 1 : 0;
-                }
-            } else {
-                ch->status = flag ? flag : DQMC_ST_NONFINITE;
-                ch->sign = 0.0;
-                ch->bvalid = 0;
-                ch->pvalid = 0;
-                ch->svalid = 0;
+        for (int sw = 0; sw < nsweeps; ++sw) {
+            if (threadIdx.x == 0) {
+                for (int i = 0; i < 4; ++i) rng[i] = ch->rng[i];
+                att = 0;
+                acc = 0;
+                ch->meas_accepted = ch->accepted;
+                ch->meas_attempts = ch->attempts;
             }
-        }
-        __syncthreads();
-        if (!ok || flag) break;
-    }
+            __syncthreads();
+            const bool back = ch->alt && ch->dir;
+            bool ok = back ? sweep_body_back(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr)
+                           : sweep_body(ch, md, kflags, s, &flag, rng, &att, &acc, ch->scr);
+            __syncthreads();
 #if DQMC_MINB == 1
-    if (s.spl) spl_teardown(&spl);
+            if (s.spl && spl.err) {   /* a split product was abandoned */
+                ok = false;
+                if (threadIdx.x == 0) flag |= DQMC_ST_TIMEOUT;
+                __syncthreads();
+            }
 #endif
+            if (threadIdx.x == 0) {
+                for (int i = 0; i < 4; ++i) ch->rng[i] = rng[i];
+                ch->attempts += att;
+                ch->accepted += acc;
+                if (ok && !flag) {
+                    ch->sweeps++;
+                    ch->bvalid = 1;
+                    if (ch->alt) {   /* dqmc.c:806-810, 943-946 */
+                        ch->dir = back ? 0 : 1;
+                        ch->pvalid = back ? 0 : 1;
+                        ch->svalid = back ? 1 : 0;
+                    }
+                } else {
+                    ch->status = flag ? flag : DQMC_ST_NONFINITE;
+                    ch->sign = 0.0;
+                    ch->bvalid = 0;
+                    ch->pvalid = 0;
+                    ch->svalid = 0;
+                }
+            }
+            __syncthreads();
+            if (!ok || flag) break;
+        }
+#if DQMC_MINB == 1
+        if (s.spl) spl_teardown(&spl);
+#endif
+    }
+    /* the one exit of rank 0: release the other ranks */
+    if (cc > 1) {
+        if (threadIdx.x == 0) ch->cl.op = CL_EXIT;
+        cl_sync();
+    }
 }
 
 /* G from scratch at l0 = 0 for every chain (dqmc_init_modes, dqmc.c:466-483). */
@@ -1252,6 +1374,47 @@ inline void launch_sweep(unsigned nc, size_t smem, cudaStream_t st, DqmcChainDev
                          const DqmcModelDev *m, int flags, int nsweeps, const int *order)
 {
     k_sweep<<<nc, NT, smem, st>>>(c, m, flags, nsweeps, order);
+}
+
+/* The sweep kernel with one cluster of cc CTAs per chain (cl_serve). */
+inline cudaLaunchConfig_t cluster_config(unsigned nc, int cc, size_t smem, cudaStream_t st,
+                                         cudaLaunchAttribute *at)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nc * (unsigned)cc, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cc;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+/* How many clusters of cc CTAs (smem bytes each) the device holds at once
+ * (0: such a cluster cannot be resident). */
+inline cudaError_t cluster_fit(int cc, size_t smem, int *nclusters)
+{
+    *nclusters = 0;
+    cudaError_t e = cudaSuccess;
+    if (cc > 8)
+        e = cudaFuncSetAttribute(k_sweep, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = cluster_config(1, cc, smem, nullptr, at);
+    return cudaOccupancyMaxActiveClusters(nclusters, (void *)k_sweep, &cfg);
+}
+
+inline cudaError_t launch_sweep_cluster(unsigned nc, int cc, size_t smem, cudaStream_t st,
+                                        DqmcChainDev *c, const DqmcModelDev *m, int flags,
+                                        int nsweeps, const int *order)
+{
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = cluster_config(nc, cc, smem, st, at);
+    return cudaLaunchKernelEx(&cfg, k_sweep, c, m, flags, nsweeps, order);
 }
 
 inline void launch_measure(unsigned nc, size_t msmem, cudaStream_t st, DqmcChainDev *c,
