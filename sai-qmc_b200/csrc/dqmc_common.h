@@ -102,6 +102,12 @@ typedef struct {
 
 /* largest cluster that advances one chain (non-portable size above 8)     */
 #define DQMC_MAX_CHAIN_CTAS 16
+/* per-chain global staging for the other ranks of a chain's cluster: a site
+ * block's flush operands (four DQMC_MAX_KB x (DQMC_MAX_KB + 2) blocks, the
+ * DQMC_MAX_KB factors and the accepted list), then the pre-pivot's column
+ * norms (DQMC_MAX_N)                                                     */
+#define DQMC_CL_FLUSH_DOUBLES (4 * DQMC_MAX_KB * (DQMC_MAX_KB + 2) + 2 * DQMC_MAX_KB)
+#define DQMC_CL_STAGE_DOUBLES (DQMC_CL_FLUSH_DOUBLES + DQMC_MAX_N)
 
 typedef struct {
     int model, n, L, stab, M, kb;
@@ -157,6 +163,7 @@ typedef struct {
      * rebuilds from scratch, measurements */
     unsigned long long pcalls[DQMC_PH_COUNT];
     DqmcClCmd cl;
+    double *clstage;           /* DQMC_CL_STAGE_DOUBLES */
 } DqmcChainDev;
 
 /* UDV slot: U (n*n) | T (n*n) | ell = log D (n) | detU (1) | pad (1)        */

@@ -572,6 +572,7 @@ struct Smem {
      * block through which rank 0 hands the others a product */
     Part cl;
     DqmcClCmd *cmd;
+    double *stage;   /* the chain's DQMC_CL_STAGE_DOUBLES global staging */
 };
 
 __host__ __device__ inline size_t smem_doubles(int n, int kb)
@@ -624,6 +625,7 @@ __device__ inline Smem carve(double *base, int n, int kb)
     s.spl = nullptr;
     s.cl = Part();
     s.cmd = nullptr;
+    s.stage = nullptr;
     return s;
 }
 
@@ -649,7 +651,8 @@ enum {
     CL_QRIGHT,      /* qr_apply_right_sm: row blocks                   */
     CL_TRSM,        /* trsm_upper: column ranges                       */
     CL_UGEMM,       /* the UDV updates' products (udv_gemm kinds)      */
-    CL_ZY           /* flush_zy: row and column ranges                 */
+    CL_ZY,          /* flush_zy: row and column ranges                 */
+    CL_PREPIV       /* prepivot: column norms and the gather by columns */
 };
 
 __device__ __forceinline__ void cl_sync()
@@ -1022,8 +1025,74 @@ __device__ __noinline__ void trsm_upper(int n, const double *A, const double *Y,
 /* ------------------------------------------------- pre-pivoted factor */
 /* Column pivoting by a one-time norm sort (pre-pivoting): perm[r] is the
  * column of M with the r-th largest 2-norm; Aout[:, r] = M[:, perm[r]]. */
+/* prepivot as a split command of a cluster per chain: the ranks share the
+ * columns' norms (same per-column arithmetic, through the chain's global
+ * staging; a norm that would raise the non-finite flag travels as NaN and
+ * rank 0 raises it), every rank forms the same order, and the ranks gather
+ * a range of columns each.  flag: rank 0's (unused elsewhere). */
+__device__ __noinline__ void prepivot_cl(int n, const double *M, double *Aout, Smem &s,
+                                         int *flag)
+{
+    cl_post(s, CL_PREPIV, M, Aout, nullptr, nullptr, nullptr, nullptr, n, 0, 0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *nst = s.stage + DQMC_CL_FLUSH_DOUBLES;
+    double *nrm = s.vD;
+    for (int c = s.cl.r * NW + warp; c < n; c += s.cl.c * NW) {
+        double mx = 0.0;
+        for (int r = lane; r < n; r += 32) mx = fmax(mx, fabs(M[r + (size_t)c * n]));
+        mx = warp_max(mx);
+        double sq = 0.0;
+        if (mx > 0.0 && isfinite(mx)) {
+            const double inv = 1.0 / mx;
+            for (int r = lane; r < n; r += 32) {
+                const double x = M[r + (size_t)c * n] * inv;
+                sq += x * x;
+            }
+        }
+        sq = warp_sum(sq);
+        if (lane == 0) {
+            double v = (mx > 0.0) ? log(mx) + 0.5 * log(sq) : -INFINITY;
+            if (!isfinite(mx) || isnan(v)) v = NAN;
+            nst[c] = v;
+        }
+    }
+    cl_sync();
+    bool bad = false;
+    for (int c = threadIdx.x; c < n; c += NT) {
+        double v = nst[c];
+        if (isnan(v)) {
+            bad = true;
+            v = -INFINITY;
+        }
+        nrm[c] = v;
+    }
+    if (bad && s.cl.r == 0) raise_flag(flag, DQMC_ST_NONFINITE);
+    __syncthreads();
+    for (int c = threadIdx.x; c < n; c += NT) {
+        const double v = nrm[c];
+        int rank = 0;
+        for (int d = 0; d < n; ++d) {
+            const double w = nrm[d];
+            rank += (w > v) || (w == v && d < c);
+        }
+        s.perm[rank] = c;
+    }
+    __syncthreads();
+    int lo, hi;
+    part_range(s, n, lo, hi);
+    for (int e = lo * n + threadIdx.x; e < hi * n; e += NT) {
+        const int i = e % n, r = e / n;
+        Aout[e] = M[i + (size_t)s.perm[r] * n];
+    }
+    cl_done(s);
+}
+
 __device__ __noinline__ void prepivot(int n, const double *M, double *Aout, Smem &s, int *flag)
 {
+    if (s.cl.c > 1) {
+        prepivot_cl(n, M, Aout, s, flag);
+        return;
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *nrm = s.vD;
     for (int c = warp; c < n; c += NW) {

@@ -702,6 +702,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         off += rup((size_t)e->nbin * m.nq_perp * 8 + 8);
         if (mixed) off += 2 * spl_bytes(n);
         if (e->desc.green_log > 0) off += rup((size_t)e->desc.green_log * nn * 8);
+        off += rup((size_t)DQMC_CL_STAGE_DOUBLES * 8);       /* cluster staging */
         const size_t sm = dq::smem_bytes(n, c.kb);
         if (sm > maxsmem) maxsmem = sm;
         const size_t sm2 = dq2x::smem_bytes(n, c.kb);
@@ -780,6 +781,7 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
             d.glog_cap = e->desc.green_log;
             d.glog = (double *)take((size_t)d.glog_cap * nn * 8);
         }
+        d.clstage = (double *)take((size_t)DQMC_CL_STAGE_DOUBLES * 8);
         CU(cudaMemcpy(d.field, c.field.data(), c.field.size(), cudaMemcpyHostToDevice));
     }
     e->dchains = (DqmcChainDev *)(e->darena + cstruct);

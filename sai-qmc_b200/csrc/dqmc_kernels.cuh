@@ -61,29 +61,55 @@ __device__ __forceinline__ Scr chain_scr(const DqmcChainDev *ch)
 /* Zs_B rows and Ys_B columns of a site block's flush (block_flush, after
  * the inverses): TuP, facs and the pair-staging operands TvP, Qa, PaT (in
  * the GEMM staging area) and the accepted list are in shared memory.  Rows
- * and columns are independent: a split command of a cluster per chain,
- * whose other ranks take those small operands from rank 0's shared memory
- * and form a contiguous range of rows and columns each. */
+ * and columns are independent: a split command of a cluster per chain.
+ * Rank 0 copies those small operands to the chain's global staging area
+ * before posting (`stage`, DQMC_CL_STAGE_DOUBLES; the other ranks read it
+ * from L2 into the same shared-memory places, rather than all reading rank
+ * 0's shared memory at once), and every rank forms a contiguous range of
+ * rows and columns. */
 __device__ __noinline__ void flush_zy(int n, int i0, int m, int mA, const double *G, double *Zs,
                                       double *Ys, int ldy, const double *TuP,
-                                      const double *facs, Smem &s)
+                                      const double *facs, double *stage, Smem &s)
 {
     constexpr int KB = DQMC_MAX_KB;
     constexpr int LT = KB + 2;
     const int tid = threadIdx.x;
-    cl_post(s, CL_ZY, G, Zs, Ys, TuP, facs, nullptr, n, i0, m | (mA << 8) | (ldy << 16));
     double *TvP = s.gsm + 2 * KB * LT, *YA = s.gsm + KB * LT, *ZA = s.gsm;
     const int *alist = s.iscr;
-    if (s.cl.r > 0) {
-        cl_pull(const_cast<double *>(TuP), KB * LT);
-        cl_pull(TvP, KB * LT);
-        cl_pull(const_cast<double *>(facs), KB);
-        cl_pull(s.iscr, KB);
-        if (mA > 0) {
-            cl_pull(YA, KB * LT);
-            cl_pull(ZA, KB * LT);
+    if (s.cl.c > 1) {
+        /* stage: TuP | TvP | YA | ZA (KB x LT each) | facs | accepted list */
+        double *tuS = stage, *tvS = stage + KB * LT, *yaS = stage + 2 * KB * LT,
+               *zaS = stage + 3 * KB * LT, *fS = stage + 4 * KB * LT;
+        int *aS = reinterpret_cast<int *>(fS + KB);
+        const int nblk = mA > 0 ? 4 : 2;
+        double *tuL = const_cast<double *>(TuP), *fL = const_cast<double *>(facs);
+        int *aL = s.iscr;
+        auto src = [=](int e) -> const double * {
+            const int b = e / (KB * LT), o = e % (KB * LT);
+            return b == 0 ? tuL + o : b == 1 ? TvP + o : b == 2 ? YA + o : ZA + o;
+        };
+        auto dst = [=](int e) -> double * {
+            const int b = e / (KB * LT), o = e % (KB * LT);
+            return b == 0 ? tuS + o : b == 1 ? tvS + o : b == 2 ? yaS + o : zaS + o;
+        };
+        if (s.cl.r == 0) {
+            ew_batched(nblk * KB * LT, [=](int e) { return *src(e); },
+                       [=](int e, double x) { *dst(e) = x; });
+            for (int e = tid; e < KB; e += NT) {
+                fS[e] = fL[e];
+                aS[e] = aL[e];
+            }
         }
-        __syncthreads();
+        cl_post(s, CL_ZY, G, Zs, Ys, TuP, facs, stage, n, i0, m | (mA << 8) | (ldy << 16));
+        if (s.cl.r > 0) {
+            ew_batched(nblk * KB * LT, [=](int e) { return *dst(e); },
+                       [=](int e, double x) { *const_cast<double *>(src(e)) = x; });
+            for (int e = tid; e < KB; e += NT) {
+                fL[e] = fS[e];
+                aL[e] = aS[e];
+            }
+            __syncthreads();
+        }
     }
     int lo, hi;
     part_range(s, n, lo, hi);
@@ -272,7 +298,8 @@ __device__ __noinline__ void cl_serve(Smem &s)
         const int op = c->op;
         if (op == CL_EXIT) break;
         const int i0 = c->i[0], i1 = c->i[1], i2 = c->i[2];
-        const void *p0 = c->p[0], *p1 = c->p[1], *p2 = c->p[2], *p3 = c->p[3], *p4 = c->p[4];
+        const void *p0 = c->p[0], *p1 = c->p[1], *p2 = c->p[2], *p3 = c->p[3], *p4 = c->p[4],
+                   *p5 = c->p[5];
         const double d0 = c->d[0], d1 = c->d[1], d2 = c->d[2], d3 = c->d[3];
         switch (op) {
         case CL_WRAP:
@@ -306,9 +333,13 @@ __device__ __noinline__ void cl_serve(Smem &s)
         case CL_UGEMM:
             udv_gemm(i1, i0, (const double *)p0, (const double *)p1, (double *)p2, s);
             break;
+        case CL_PREPIV:
+            prepivot_cl(i0, (const double *)p0, (double *)p1, s, nullptr);
+            break;
         case CL_ZY:
             flush_zy(i0, i1, i2 & 255, (i2 >> 8) & 255, (const double *)p0, (double *)p1,
-                     (double *)p2, i2 >> 16, (const double *)p3, (const double *)p4, s);
+                     (double *)p2, i2 >> 16, (const double *)p3, (const double *)p4,
+                     (double *)p5, s);
             break;
         default:
             break;
@@ -404,7 +435,7 @@ __device__ __noinline__ int block_flush(int n, int kb, int i0, int m, double *G,
     }
     __syncthreads();
     pc.charge(ch, DQMC_PH_FLUSH);
-    flush_zy(n, i0, m, mA, G, Zs, Ys, ldy, TuP, facs, s);
+    flush_zy(n, i0, m, mA, G, Zs, Ys, ldy, TuP, facs, ch->clstage, s);
     const int mt = mA + m;
     if (!flush) {
         pc.charge(ch, DQMC_PH_FLUSH);
@@ -1050,6 +1081,7 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     Smem s = carve(smraw, ch->n, ch->kb);
     s.cl = Part{cr, cc};
     s.cmd = &ch->cl;
+    s.stage = ch->clstage;
     if (cr > 0) {
         cl_serve(s);
         return;
