@@ -571,9 +571,10 @@ def run_gpu_arm(args):
     chains = args.chains or 2 * props.multi_processor_count
     precision = dq.PREC_MIXED if args.precision == "mixed" else dq.PREC_FP64
     eng = make_engine(dq, chains, rank * chains, precision, device=local,
-                      ctas_per_sm=args.ctas_per_sm)
+                      ctas_per_sm=args.ctas_per_sm, chain_ctas=args.chain_ctas)
     nbin = max(1, args.steps)
     eng.prepare(nbin)
+    per_sm, chain_ctas = eng.residency()
     for w in range(args.warmup):
         eng.sweep_measure(1, 0)
     eng.sync()
@@ -668,6 +669,7 @@ def run_gpu_arm(args):
             "config": {"workload": workload_name(chains), "chains_per_gpu": chains,
                        "n": N_SITES, "L": L_SLICES, "stab": STAB, "delay_rank": KB,
                        "precision": args.precision,
+                       "residency": {"chains_per_sm": per_sm, "ctas_per_chain": chain_ctas},
                        "l2": f"inputs larger than L2: {chains} chains x ~21 MB resident "
                              f"state >> {L2_BYTES // 2**20} MB L2",
                        "parallelism": f"replicas x{world} (no collective on the data path)"},
@@ -746,6 +748,8 @@ def main():
     ap.add_argument("--c3-sigma", action="store_true",
                     help="also run the single-chain 100/400/20 workload in both precisions "
                          "and report each observable's difference in FP64 error bars")
+    ap.add_argument("--chain-ctas", type=int, default=0,
+                    help="CTAs per chain of the main line's engine (0: automatic)")
     ap.add_argument("--ctas-per-sm", type=int, default=0, choices=[0, 1, 2],
                     help="sweep kernel residency (0: automatic)")
     args = ap.parse_args()
