@@ -119,17 +119,17 @@ typedef struct {
     int chain_ctas;  /* CTAs that advance one chain together as a thread-block
                         cluster, 2..16 (above 8 where the device allows a
                         non-portable cluster size); 1 = one CTA per chain;
-                        0 = automatic: for FP64 batches of fewer chains
-                        than SMs with a lattice of n >= 128, the largest
+                        0 = automatic: for batches of fewer chains than
+                        SMs with a lattice of n >= 128, the largest
                         size at which all the batch's clusters are resident
                         at once, else 1.  Rank 0 runs the sweep; every rank
                         forms its share of the output tiles of the wrap,
                         the B-block products and the delayed-update G
-                        update, so the trajectory equals the one-CTA run
-                        bit for bit.  For batches of fewer chains than SMs
-                        (one chain, a few large lattices).  FP64 only; one
-                        CTA per SM.  No counterpart in the reference, whose
-                        sweep runs on one host thread.                       */
+                        update (FP64 or split products), so the trajectory
+                        equals the one-CTA run bit for bit.  For batches of
+                        fewer chains than SMs (one chain, a few large
+                        lattices); one CTA per SM.  No counterpart in the
+                        reference, whose sweep runs on one host thread.     */
     int reserved;
 } dqmc_engine_desc;
 

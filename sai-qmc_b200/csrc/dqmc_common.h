@@ -96,6 +96,7 @@ typedef struct {
  * the other ranks read it after the cluster barrier. */
 typedef struct {
     int op, i[3];
+    int err, pad;              /* a rank's bounded wait ran out during the command */
     const void *p[6];
     double d[4];
 } DqmcClCmd;

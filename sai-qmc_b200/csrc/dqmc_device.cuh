@@ -652,7 +652,9 @@ enum {
     CL_TRSM,        /* trsm_upper: column ranges                       */
     CL_UGEMM,       /* the UDV updates' products (udv_gemm kinds)      */
     CL_ZY,          /* flush_zy: row and column ranges                 */
-    CL_PREPIV       /* prepivot: column norms and the gather by columns */
+    CL_PREPIV,      /* prepivot: column norms and the gather by columns */
+    CL_WSPLIT,      /* wrap_green_split: lines of each split, tiles     */
+    CL_FSPLIT       /* flush_split: lines of each split, tiles          */
 };
 
 __device__ __forceinline__ void cl_sync()

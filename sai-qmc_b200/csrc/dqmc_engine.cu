@@ -335,10 +335,6 @@ dqmc_engine *dqmc_engine_create(const dqmc_engine_desc *desc)
         set_err("chain_ctas %d is outside 0..%d", d.chain_ctas, DQMC_MAX_CHAIN_CTAS);
         return nullptr;
     }
-    if (d.chain_ctas > 1 && d.precision == DQMC_PREC_MIXED) {
-        set_err("chain_ctas %d: a cluster per chain runs the FP64 products only", d.chain_ctas);
-        return nullptr;
-    }
     if (d.chain_ctas > 1 && d.ctas_per_sm == 2) {
         set_err("chain_ctas %d needs one CTA per SM (ctas_per_sm 0 or 1)", d.chain_ctas);
         return nullptr;
@@ -827,12 +823,12 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
         if (e->per_sm == 2) CU(dq2x::set_attrs(e->smem2, e->msmem));
     }
     /* One thread-block cluster per chain.  Automatic (chain_ctas = 0) for
-     * FP64 batches of fewer chains than SMs whose largest lattice has
+     * batches of fewer chains than SMs whose largest lattice has
      * n >= 128 (below that the split products are too small to pay): the
      * largest cluster such that every chain's cluster is resident at once
      * (a second wave of clusters costs more than narrower clusters). */
     e->cl = 1;
-    if (e->desc.chain_ctas == 0 && !mixed && e->per_sm == 1 && maxn >= 128) {
+    if (e->desc.chain_ctas == 0 && e->per_sm == 1 && maxn >= 128) {
         static const int sizes[] = {16, 12, 8, 6, 4, 3, 2};
         for (int cc : sizes) {
             if ((long)nc * cc > nsm) continue;

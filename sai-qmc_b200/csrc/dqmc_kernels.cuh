@@ -336,6 +336,17 @@ __device__ __noinline__ void cl_serve(Smem &s)
         case CL_PREPIV:
             prepivot_cl(i0, (const double *)p0, (double *)p1, s, nullptr);
             break;
+#if DQMC_MINB == 1
+        case CL_WSPLIT:
+            wrap_green_split(i0, (double *)p0, (double *)p1, *(const DqmcModelDev *)p2,
+                             (const DqmcChainDev *)p3, (const signed char *)p4, d0, d1, d2, d3,
+                             i1 != 0, s);
+            break;
+        case CL_FSPLIT:
+            flush_split(i0, i1, (double *)p0, (const double *)p1, (const double *)p2, i2,
+                        (const DqmcChainDev *)p3, s);
+            break;
+#endif
         case CL_ZY:
             flush_zy(i0, i1, i2 & 255, (i2 >> 8) & 255, (const double *)p0, (double *)p1,
                      (double *)p2, i2 >> 16, (const double *)p3, (const double *)p4,
@@ -1082,16 +1093,30 @@ __global__ void __launch_bounds__(NT, DQMC_MINB)
     s.cl = Part{cr, cc};
     s.cmd = &ch->cl;
     s.stage = ch->clstage;
+#if DQMC_MINB == 1
+    __shared__ SplCtx spl;
+#endif
     if (cr > 0) {
+#if DQMC_MINB == 1
+        if (kflags & KF_MIXED) {   /* this rank's own tensor memory */
+            spl_setup(&spl);
+            s.spl = &spl;
+        }
+#endif
         cl_serve(s);
+#if DQMC_MINB == 1
+        if (s.spl) spl_teardown(&spl);
+#endif
         return;
     }
-    if (threadIdx.x == 0) flag = ch->status;
+    if (threadIdx.x == 0) {
+        flag = ch->status;
+        ch->cl.err = 0;
+    }
     __syncthreads();
     if (!flag) {
 #if DQMC_MINB == 1
-        __shared__ SplCtx spl;
-        if ((kflags & KF_MIXED) && cc == 1) {
+        if (kflags & KF_MIXED) {
             spl_setup(&spl);
             s.spl = &spl;
         }

@@ -226,10 +226,15 @@ __device__ __forceinline__ void spl_tr4(uint32_t a, uint32_t b, uint32_t c, uint
  * pass gives consecutive threads consecutive lines of one 16-entry k group
  * (coalesced 16-byte stores), two groups in flight per thread. */
 template <bool KCONTIG, class LD>
-__device__ __noinline__ void spl_split(int lines, int K, LD ld, SplitOp op)
+__device__ __noinline__ void spl_split(int lines, int K, LD ld, SplitOp op, Part pt = Part())
 {
     const int tid = threadIdx.x;
-    const int lpad = op.nlb * SPL_LB;
+    const int lpad_all = op.nlb * SPL_LB;
+    /* this CTA's lines [l0, l0 + lpad) (all of them unless a cluster shares
+     * the split; each line's scale and digits depend on that line alone) */
+    const int per = (lpad_all + pt.c - 1) / pt.c;
+    const int l0 = min(lpad_all, pt.r * per);
+    const int lpad = min(lpad_all, l0 + per) - l0;
     auto set_line = [&](int l, double m) {
         int e = 0;
         if (m > 0.0 && isfinite(m)) frexp(m, &e);
@@ -240,7 +245,7 @@ __device__ __noinline__ void spl_split(int lines, int K, LD ld, SplitOp op)
     };
     if (KCONTIG) {
         /* a thread per line; 16 entries (128 contiguous bytes) per step */
-        for (int l = tid; l < lpad; l += NT) {
+        for (int l = l0 + tid; l < l0 + lpad; l += NT) {
             double m = 0.0;
             if (l < lines) {
                 int k = 0;
@@ -259,7 +264,7 @@ __device__ __noinline__ void spl_split(int lines, int K, LD ld, SplitOp op)
             set_line(l, m);
         }
     } else {
-        for (int l = tid; l < lpad; l += NT) {
+        for (int l = l0 + tid; l < l0 + lpad; l += NT) {
             double m = 0.0;
             if (l < lines) {
                 /* sixteen independent loads in flight per step */
@@ -289,7 +294,7 @@ __device__ __noinline__ void spl_split(int lines, int K, LD ld, SplitOp op)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int it = it0 + h * NT;
-            ll[h] = it % lpad;
+            ll[h] = l0 + (lpad > 0 ? it % lpad : 0);
             gg[h] = it < items ? it / lpad : -1;
 #pragma unroll
             for (int u = 0; u < 16; ++u) {
@@ -435,15 +440,18 @@ struct EpiDiag {      /* C = diag(r) (A B) diag(q) */
  * false when a wait ran out (cx->err set; nothing further is issued). */
 template <class EPI>
 __device__ __noinline__ bool spl_gemm(int M, int N, SplitOp A, SplitOp B, EPI epi,
-                                      unsigned char *sm, SplCtx *cx)
+                                      unsigned char *sm, SplCtx *cx, Part pt = Part())
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tm = (M + SPL_LB - 1) / SPL_LB, tn = (N + SPL_N - 1) / SPL_N, nk = A.nkc;
-    const int ntile = tm * tn;
+    /* this CTA's tiles pt.r, pt.r + pt.c, ... (all of them by default) */
+    const int ntile = tm * tn > pt.r ? (tm * tn - pt.r + pt.c - 1) / pt.c : 0;
     const unsigned total = (unsigned)ntile * 2 * nk;
     /* earlier generic-proxy use of the staging area is ordered before the
-     * bulk copies that overwrite it */
+     * bulk copies that overwrite it; operands split by other CTAs of a
+     * cluster (published by the cluster barrier) before the bulk reads */
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("fence.proxy.async.global;" ::: "memory");
     __syncthreads();
     if (cx->err) return false;
     const uint32_t sbase = smem_u32(sm);
@@ -458,7 +466,8 @@ __device__ __noinline__ bool spl_gemm(int M, int N, SplitOp A, SplitOp B, EPI ep
             cx->err = 1;
             return;
         }
-        const int it = (int)(x / (2 * nk)), pass = (int)((x / nk) & 1), ik = (int)(x % nk);
+        const int it = pt.r + pt.c * (int)(x / (2 * nk)), pass = (int)((x / nk) & 1),
+                  ik = (int)(x % nk);
         const uint32_t bytes = (pass ? SPL_S : SPL_ACC) * SPL_SLICE;
         const signed char *ga = A.t + ((size_t)(it % tm) * A.nkc + ik) * (size_t)SPL_TILE;
         const signed char *gb = B.t + ((size_t)(it / tm) * B.nkc + ik) * (size_t)SPL_TILE;
@@ -473,7 +482,7 @@ __device__ __noinline__ bool spl_gemm(int M, int N, SplitOp A, SplitOp B, EPI ep
     if (tid == 0)
         for (unsigned x = 0; x + 1 < SPL_NSTAGE && x < total && !cx->err; ++x) issue(x);
     for (int t = 0; t < ntile; ++t) {
-        const int mb = t % tm, nb = t / tm;
+        const int gt = pt.r + pt.c * t, mb = gt % tm, nb = gt / tm;
         for (int pass = 0; pass < 2; ++pass) {
             if (tid == 0) {
                 tc_fence_after();
@@ -582,15 +591,36 @@ __device__ __noinline__ bool spl_gemm(int M, int N, SplitOp A, SplitOp B, EPI ep
     return !cx->err;
 }
 
+/* End of a split product as a command of a cluster per chain: a rank whose
+ * bounded wait ran out reports it in the command block, rank 0 takes it
+ * into its own error state after the last barrier. */
+__device__ __forceinline__ bool spl_cl_finish(Smem &s, SplCtx *cx)
+{
+    if (s.cl.c > 1) {
+        if (s.cl.r > 0 && threadIdx.x == 0 && cx->err) atomicOr(&s.cmd->err, 1);
+        cl_done(s);
+        if (s.cl.r == 0 && threadIdx.x == 0 && *(volatile int *)&s.cmd->err) cx->err = 1;
+        __syncthreads();
+    }
+    return !cx->err;
+}
+
 /* G <- B_l G B_l^-1 (green_wrap, green.c:509-527) or, back, G <- B_l^-1
  * G B_l (green_wrap_backward, green.c:529-548), both products split:
  * forward P = [diag(v) G diag(1/v)] expK^-1, G = expK P; backward
- * P = G expK, G = diag(1/v) (expK^-1 P) diag(v).  P: n x n scratch. */
+ * P = G expK, G = diag(1/v) (expK^-1 P) diag(v).  P: n x n scratch.
+ * A split command with a cluster per chain: the ranks split a range of
+ * lines of each operand and form a share of the output tiles, each on its
+ * own tensor memory; the per-tile arithmetic is the one-CTA product's.
+ * Every rank runs every step (a failed wait makes the later products
+ * return at once) so the ranks stay in step. */
 __device__ __noinline__ bool wrap_green_split(int n, double *G, double *P, const DqmcModelDev &md,
                                               const DqmcChainDev *ch, const signed char *fl,
                                               double v0, double v1, double vi0, double vi1,
                                               bool back, Smem &s)
 {
+    cl_post(s, CL_WSPLIT, G, P, &md, ch, fl, nullptr, n, back ? 1 : 0, 0, v0, v1, vi0, vi1);
+    const Part pt = s.cl;
     double *vv = s.vA, *vi = s.vB;
     for (int k = threadIdx.x; k < n; k += NT) {
         const bool up = fl[k] > 0;
@@ -604,29 +634,42 @@ __device__ __noinline__ bool wrap_green_split(int n, double *G, double *P, const
     a.nkc = b.nkc = spl_nkc(n);
     if (!back) {
         spl_split<false>(
-            n, n, [=](int k, int l) { return (vv[l] * G[l + (size_t)k * n]) * vi[k]; }, a);
-        if (!spl_gemm(n, n, a, md.spKi_c, EpiStore{P, n}, sm, cx)) return false;
-        spl_split<true>(n, n, [=](int k, int l) { return P[k + (size_t)l * n]; }, b);
-        return spl_gemm(n, n, md.spK_r, b, EpiStore{G, n}, sm, cx);
+            n, n, [=](int k, int l) { return (vv[l] * G[l + (size_t)k * n]) * vi[k]; }, a, pt);
+        part_sync(s);
+        spl_gemm(n, n, a, md.spKi_c, EpiStore{P, n}, sm, cx, pt);
+        part_sync(s);
+        spl_split<true>(n, n, [=](int k, int l) { return P[k + (size_t)l * n]; }, b, pt);
+        part_sync(s);
+        spl_gemm(n, n, md.spK_r, b, EpiStore{G, n}, sm, cx, pt);
+    } else {
+        spl_split<false>(n, n, [=](int k, int l) { return G[l + (size_t)k * n]; }, a, pt);
+        part_sync(s);
+        spl_gemm(n, n, a, md.spK_c, EpiStore{P, n}, sm, cx, pt);
+        part_sync(s);
+        spl_split<true>(n, n, [=](int k, int l) { return P[k + (size_t)l * n]; }, b, pt);
+        part_sync(s);
+        spl_gemm(n, n, md.spKi_r, b, EpiDiag{G, n, vi, vv}, sm, cx, pt);
     }
-    spl_split<false>(n, n, [=](int k, int l) { return G[l + (size_t)k * n]; }, a);
-    if (!spl_gemm(n, n, a, md.spK_c, EpiStore{P, n}, sm, cx)) return false;
-    spl_split<true>(n, n, [=](int k, int l) { return P[k + (size_t)l * n]; }, b);
-    return spl_gemm(n, n, md.spKi_r, b, EpiDiag{G, n, vi, vv}, sm, cx);
+    return spl_cl_finish(s, cx);
 }
 
 /* G -= Zs Ys, rank mt (green_delay_flush, green.c:462-475, through
  * la_gemm_nt_rect, linalg.c:209-219) as a split product; Zs n x mt (ld n),
- * Ys mt x n (ld ldy). */
+ * Ys mt x n (ld ldy).  A split command with a cluster per chain (as the
+ * wrap). */
 __device__ __noinline__ bool flush_split(int n, int mt, double *G, const double *Zs,
                                          const double *Ys, int ldy, const DqmcChainDev *ch,
                                          Smem &s)
 {
+    cl_post(s, CL_FSPLIT, G, Zs, Ys, ch, nullptr, nullptr, n, mt, ldy);
+    const Part pt = s.cl;
     SplitOp a = ch->spA, b = ch->spB;
     a.nkc = b.nkc = spl_nkc(mt);
-    spl_split<false>(n, mt, [=](int k, int l) { return Zs[l + (size_t)k * n]; }, a);
-    spl_split<true>(n, mt, [=](int k, int l) { return Ys[k + (size_t)l * ldy]; }, b);
-    return spl_gemm(n, n, a, b, EpiSub{G, n}, (unsigned char *)s.gsm, (SplCtx *)s.spl);
+    spl_split<false>(n, mt, [=](int k, int l) { return Zs[l + (size_t)k * n]; }, a, pt);
+    spl_split<true>(n, mt, [=](int k, int l) { return Ys[k + (size_t)l * ldy]; }, b, pt);
+    part_sync(s);
+    spl_gemm(n, n, a, b, EpiSub{G, n}, (unsigned char *)s.gsm, (SplCtx *)s.spl, pt);
+    return spl_cl_finish(s, (SplCtx *)s.spl);
 }
 
 #endif  /* DQMC_MINB == 1 */

@@ -107,18 +107,29 @@ def test_cluster_matches_reference_golden():
     eng.close()
 
 
+@pytest.mark.parametrize("ctas", [4, 16])
+def test_cluster_mixed_precision_equals_one_cta(ctas):
+    """Split products (tcgen05 kind::i8) shared over the cluster: each rank
+    splits a range of lines and forms a share of the tiles on its own tensor
+    memory; the same digits and tiles as one CTA."""
+    run_pair([(16, 16, None)], 16, 8, [11], ctas, precision=dq.PREC_MIXED)
+
+
+def test_cluster_mixed_precision_alternating_uneven():
+    run_pair([(8, 8, None), (12, 12, None)], 20, 5, [3, 4], 4, sweeps=4,
+             precision=dq.PREC_MIXED, sweep_order=dq.SWEEP_ALTERNATING)
+
+
 def test_cluster_rejects_bad_settings():
     with pytest.raises(dq.DqmcError, match="chain_ctas"):
         dq.Engine(chain_ctas=17)
-    with pytest.raises(dq.DqmcError, match="FP64"):
-        dq.Engine(chain_ctas=4, precision=dq.PREC_MIXED)
     with pytest.raises(dq.DqmcError, match="one CTA per SM"):
         dq.Engine(chain_ctas=4, ctas_per_sm=2)
 
 
 def test_cluster_size_chosen_automatically():
-    """chain_ctas = 0: a cluster per chain for FP64 batches of fewer chains
-    than SMs with n >= 128, one CTA per chain otherwise."""
+    """chain_ctas = 0: a cluster per chain for batches of fewer chains than
+    SMs with n >= 128, one CTA per chain otherwise."""
     def residency(Lx, nch, **kw):
         T, bp = dq.square_lattice(Lx, Lx)
         e = dq.Engine(**kw)
@@ -132,7 +143,7 @@ def test_cluster_size_chosen_automatically():
     per_sm, cc = residency(16, 1)
     assert per_sm == 1 and cc > 1
     assert residency(16, 1, chain_ctas=1) == (1, 1)
-    assert residency(16, 1, precision=dq.PREC_MIXED) == (1, 1)
+    assert residency(16, 1, precision=dq.PREC_MIXED)[1] == cc
     assert residency(8, 1) == (1, 1)
     per_sm, cc4 = residency(16, 8)
     assert per_sm == 1 and 1 < cc4 <= cc
