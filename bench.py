@@ -456,7 +456,7 @@ def batch_line(dq, kind, precision, sweeps, peak, tuned=False):
     eng.mark(1)
     ms = eng.elapsed_ms() / sweeps
     c1 = [eng.counters(c) for c in range(len(chains))]
-    chain_ctas = eng.residency()[1]
+    _, chain_ctas, cluster_chains = eng.residency()
     eng.close()
     upd = sum(w["n"] * w["L"] for w in chains)
     flops = sum(flops_per_chain_sweep(w["n"], w["L"], w["stab"],
@@ -488,7 +488,7 @@ def batch_line(dq, kind, precision, sweeps, peak, tuned=False):
             "chains": len(chains), "field_updates_per_sweep": upd,
             "precision": "mixed" if precision == dq.PREC_MIXED else "fp64",
             "chains_failed": sum(1 for c in c1 if c["status"] != 0),
-            "chain_ctas": chain_ctas,
+            "chain_ctas": chain_ctas, "chains_on_a_cluster": cluster_chains,
             "setup_and_first_sweep_s": setup_s,
             "critical_chain": crit_line,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak,
@@ -574,7 +574,7 @@ def run_gpu_arm(args):
                       ctas_per_sm=args.ctas_per_sm, chain_ctas=args.chain_ctas)
     nbin = max(1, args.steps)
     eng.prepare(nbin)
-    per_sm, chain_ctas = eng.residency()
+    per_sm, chain_ctas, cluster_chains = eng.residency()
     for w in range(args.warmup):
         eng.sweep_measure(1, 0)
     eng.sync()
@@ -669,7 +669,8 @@ def run_gpu_arm(args):
             "config": {"workload": workload_name(chains), "chains_per_gpu": chains,
                        "n": N_SITES, "L": L_SLICES, "stab": STAB, "delay_rank": KB,
                        "precision": args.precision,
-                       "residency": {"chains_per_sm": per_sm, "ctas_per_chain": chain_ctas},
+                       "residency": {"chains_per_sm": per_sm, "cluster_ctas": chain_ctas,
+                                     "chains_on_a_cluster": cluster_chains},
                        "l2": f"inputs larger than L2: {chains} chains x ~21 MB resident "
                              f"state >> {L2_BYTES // 2**20} MB L2",
                        "parallelism": f"replicas x{world} (no collective on the data path)"},

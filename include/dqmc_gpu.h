@@ -130,7 +130,11 @@ typedef struct {
                         fewer chains than SMs (one chain, a few large
                         lattices); one CTA per SM.  No counterpart in the
                         reference, whose sweep runs on one host thread.     */
-    int reserved;
+    int cluster_chains; /* with chain_ctas > 1: how many of the most
+                        expensive chains get a cluster each (0 = all); the
+                        other chains run one per CTA inside clusters of the
+                        same launch.  The automatic choice (chain_ctas = 0)
+                        sets both from a cost model of the batch.          */
 } dqmc_engine_desc;
 
 typedef struct {
@@ -237,9 +241,11 @@ int dqmc_synchronize(dqmc_engine *e);
 int dqmc_chain_count(const dqmc_engine *e);
 int dqmc_chain_dims(const dqmc_engine *e, int chain, int *n, int *L);
 /* The sweep kernel's residency chosen at dqmc_engine_prepare: chains per
- * SM (1 or 2) and CTAs per chain (1, or the cluster size).  No counterpart
- * in the reference. */
-int dqmc_engine_residency(const dqmc_engine *e, int *ctas_per_sm, int *chain_ctas);
+ * SM (1 or 2), the cluster size (1: no clusters) and how many chains, the
+ * most expensive ones, run on a cluster each.  No counterpart in the
+ * reference. */
+int dqmc_engine_residency(const dqmc_engine *e, int *ctas_per_sm, int *chain_ctas,
+                          int *cluster_chains);
 
 /* Copies back the up-spin G (n x n) at the chain's current slice (0 after a
  * sweep).  G_down = I - P G_up^T P (src/green.c:372-382). */

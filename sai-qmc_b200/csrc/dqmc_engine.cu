@@ -244,7 +244,9 @@ struct dqmc_engine {
     int nbin = 0;
     size_t smem = 0, msmem = 0, smem2 = 0;
     int per_sm = 1;           /* CTAs per SM of the sweep kernels (1 or 2) */
-    int cl = 1;               /* CTAs per chain of the sweep kernel (a cluster) */
+    int cl = 1;               /* cluster size of the sweep kernel (1: none)       */
+    int ncoop = 0;            /* chains (most expensive first) on a cluster each  */
+    int nclus = 0;            /* clusters of the launch                           */
     bool prepared = false;
     /* per-launch CUDA events (kind 0 = sweep kernel, 1 = measurement) */
     bool timing = false;
@@ -822,34 +824,78 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
                         : 1;
         if (e->per_sm == 2) CU(dq2x::set_attrs(e->smem2, e->msmem));
     }
-    /* One thread-block cluster per chain.  Automatic (chain_ctas = 0) for
-     * batches of fewer chains than SMs whose largest lattice has
-     * n >= 128 (below that the split products are too small to pay): the
-     * largest cluster such that every chain's cluster is resident at once
-     * (a second wave of clusters costs more than narrower clusters). */
+    /* Thread-block clusters.  A cluster of cc CTAs either advances one chain
+     * (the ncoop most expensive chains in launch order) or runs cc of the
+     * other chains, one per CTA.  Explicit: chain_ctas > 1, cluster_chains
+     * of them (0 = all).  Automatic (chain_ctas = 0) for batches of fewer
+     * chains than SMs whose largest lattice has n >= 128: the (cc, ncoop)
+     * whose slowest chain is predicted fastest, every cluster resident at
+     * once (a second wave of clusters costs more than narrower ones), by
+     * chain cost n^3 L (doubled on the two-spin path) over the speedup
+     * 1 + a(n) log2(cc) of a chain on cc CTAs, a(n) interpolated through
+     * measured points: (64, 0), (144, 0.245), (256, 0.30), (576, 0.67). */
     e->cl = 1;
-    if (e->desc.chain_ctas == 0 && e->per_sm == 1 && maxn >= 128) {
-        static const int sizes[] = {16, 12, 8, 6, 4, 3, 2};
-        for (int cc : sizes) {
-            if ((long)nc * cc > nsm) continue;
+    e->ncoop = (int)nc;
+    e->nclus = (int)nc;
+    {
+        std::vector<double> w(nc), an(nc);
+        std::vector<int> ord(nc);
+        CU(cudaMemcpy(ord.data(), e->dorder, sizeof(int) * nc, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < nc; ++k) {
+            const HChain &c = e->chains[ord[k]];
+            const HModel &m = e->models[c.model];
+            w[k] = (double)m.n * m.n * m.n * c.L * (m.ph ? 1.0 : 2.0);
+            static const double px[] = {64, 144, 256, 576}, py[] = {0, 0.245, 0.30, 0.67};
+            double a = py[3];
+            if (m.n <= px[0]) a = 0.0;
+            for (int q = 0; q < 3; ++q)
+                if (m.n > px[q] && m.n <= px[q + 1])
+                    a = py[q] + (py[q + 1] - py[q]) * (m.n - px[q]) / (px[q + 1] - px[q]);
+            an[k] = a;
+        }
+        auto span = [&](int cc, int k) {   /* predicted time of the slowest chain */
+            double t = 0.0;
+            for (int i = 0; i < k; ++i)
+                t = std::max(t, w[i] / (1.0 + an[i] * std::log2((double)cc)));
+            if (k < (int)nc) t = std::max(t, w[k]);
+            return t;
+        };
+        const int want = e->desc.chain_ctas;
+        if (want > 1) {
             int fit = 0;
-            if (dq::cluster_fit(cc, e->smem, &fit) != cudaSuccess) {
-                cudaGetLastError();
-                continue;
-            }
-            if (fit >= (int)nc) {
-                e->cl = cc;
-                break;
+            CU(dq::cluster_fit(want, e->smem, &fit));
+            const int k = e->desc.cluster_chains > 0 ? std::min(e->desc.cluster_chains, (int)nc)
+                                                     : (int)nc;
+            const int tot = k + ((int)nc - k + want - 1) / want;
+            if (fit < 1)
+                return set_err("dqmc_engine_prepare: a cluster of %d CTAs with %zu B of shared "
+                               "memory each cannot be resident on this device",
+                               want, e->smem);
+            e->cl = want;
+            e->ncoop = k;
+            e->nclus = tot;
+        } else if (want == 0 && e->per_sm == 1 && maxn >= 128) {
+            static const int sizes[] = {16, 12, 8, 6, 4, 3, 2};
+            double best = w.empty() ? 0.0 : w[0];
+            for (int cc : sizes) {
+                int fit = 0;
+                if (dq::cluster_fit(cc, e->smem, &fit) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                for (int k = 1; k <= (int)nc; ++k) {
+                    const int tot = k + ((int)nc - k + cc - 1) / cc;
+                    if ((long)tot * cc > nsm || tot > fit) continue;
+                    const double t = span(cc, k);
+                    if (t < 0.97 * best) {
+                        best = t;
+                        e->cl = cc;
+                        e->ncoop = k;
+                        e->nclus = tot;
+                    }
+                }
             }
         }
-    } else if (e->desc.chain_ctas > 1) {
-        int fit = 0;
-        CU(dq::cluster_fit(e->desc.chain_ctas, e->smem, &fit));
-        if (fit < 1)
-            return set_err("dqmc_engine_prepare: a cluster of %d CTAs with %zu B of shared "
-                           "memory each cannot be resident on this device",
-                           e->desc.chain_ctas, e->smem);
-        e->cl = e->desc.chain_ctas;
     }
     dq::k_init<<<(unsigned)nc, DQMC_NT, e->smem, e->stream>>>(e->dchains, e->dmodels);
     CU(cudaGetLastError());
@@ -907,8 +953,9 @@ int dqmc_sweep(dqmc_engine *e, int nsweeps)
     for (int done = 0; done < nsweeps; done += per) {
         ev_begin(e, 0);
         if (e->cl > 1)
-            CU(dq::launch_sweep_cluster(nc, e->cl, e->smem, e->stream, e->dchains, e->dmodels,
-                                        kflags(e), per, e->dorder));
+            CU(dq::launch_sweep_cluster((unsigned)e->nclus, e->cl, e->smem, e->stream,
+                                        e->dchains, e->dmodels, kflags(e), per, e->dorder,
+                                        e->ncoop, (int)nc));
         else if (e->per_sm == 2)
             dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, kflags(e), per,
                                  e->dorder);
@@ -989,8 +1036,9 @@ int dqmc_sweep_measure(dqmc_engine *e, int nsweeps, int bin)
         const int f = kflags(e) | dq::KF_MEASURE;
         ev_begin(e, 0);
         if (e->cl > 1)
-            CU(dq::launch_sweep_cluster(nc, e->cl, e->smem, e->stream, e->dchains, e->dmodels, f,
-                                        1, e->dorder));
+            CU(dq::launch_sweep_cluster((unsigned)e->nclus, e->cl, e->smem, e->stream,
+                                        e->dchains, e->dmodels, f, 1, e->dorder, e->ncoop,
+                                        (int)nc));
         else if (e->per_sm == 2)
             dq2x::launch_sweep(nc, e->smem2, e->stream, e->dchains, e->dmodels, f, 1, e->dorder);
         else
@@ -1068,11 +1116,13 @@ int dqmc_synchronize(dqmc_engine *e)
 
 int dqmc_chain_count(const dqmc_engine *e) { return e ? (int)e->chains.size() : 0; }
 
-int dqmc_engine_residency(const dqmc_engine *e, int *ctas_per_sm, int *chain_ctas)
+int dqmc_engine_residency(const dqmc_engine *e, int *ctas_per_sm, int *chain_ctas,
+                          int *cluster_chains)
 {
     if (!e || !e->prepared) return set_err("dqmc_engine_residency: engine not prepared");
     if (ctas_per_sm) *ctas_per_sm = e->per_sm;
     if (chain_ctas) *chain_ctas = e->cl;
+    if (cluster_chains) *cluster_chains = e->cl > 1 ? e->ncoop : 0;
     return 0;
 }
 

@@ -1073,21 +1073,28 @@ __device__ __noinline__ bool sweep_body_back(DqmcChainDev *ch, const DqmcModelDe
     return rebuild(0, left, false, 0);
 }
 
-/* One CTA per chain, or one thread-block cluster per chain (cl_serve);
- * order[b] names the chain of CTA (cluster) b, longest first, so a batch of
- * uneven chains does not end on a late-starting long one. */
+/* One CTA per chain, or thread-block clusters: cluster b < ncoop advances
+ * chain order[b] with all its CTAs (cl_serve); each later cluster runs cc
+ * chains, one per CTA, order[ncoop + (b - ncoop) cc + rank] (CTAs past
+ * nchains return).  order lists the chains most expensive first, so a batch
+ * of uneven chains gives its longest chains the clusters and does not end
+ * on a late-starting long one. */
 __global__ void __launch_bounds__(NT, DQMC_MINB)
     k_sweep(DqmcChainDev *chains, const DqmcModelDev *models, int kflags, int nsweeps,
-            const int *order)
+            const int *order, int ncoop, int nchains)
 {
     extern __shared__ __align__(16) double smraw[];
     __shared__ int flag;
     __shared__ uint64_t rng[4];
     __shared__ unsigned long long att, acc;
     /* a launch without clusters is a launch of one-CTA clusters */
-    const int cc = max(1, (int)cl_size_hw()), cr = cc > 1 ? (int)cl_rank_hw() : 0;
-    const int slot = (int)(blockIdx.x / (unsigned)cc);
-    DqmcChainDev *ch = &chains[order ? order[slot] : slot];
+    const int csz = max(1, (int)cl_size_hw()), crk = csz > 1 ? (int)cl_rank_hw() : 0;
+    const int slot = (int)(blockIdx.x / (unsigned)csz);
+    const bool coop = slot < ncoop;
+    const int cidx = coop ? slot : ncoop + (slot - ncoop) * csz + crk;
+    if (cidx >= nchains) return;
+    const int cc = coop ? csz : 1, cr = coop ? crk : 0;
+    DqmcChainDev *ch = &chains[order ? order[cidx] : cidx];
     const DqmcModelDev &md = models[ch->model];
     Smem s = carve(smraw, ch->n, ch->kb);
     s.cl = Part{cr, cc};
@@ -1430,7 +1437,7 @@ inline cudaError_t set_attrs(size_t smem, size_t msmem)
 inline void launch_sweep(unsigned nc, size_t smem, cudaStream_t st, DqmcChainDev *c,
                          const DqmcModelDev *m, int flags, int nsweeps, const int *order)
 {
-    k_sweep<<<nc, NT, smem, st>>>(c, m, flags, nsweeps, order);
+    k_sweep<<<nc, NT, smem, st>>>(c, m, flags, nsweeps, order, (int)nc, (int)nc);
 }
 
 /* The sweep kernel with one cluster of cc CTAs per chain (cl_serve). */
@@ -1465,13 +1472,15 @@ inline cudaError_t cluster_fit(int cc, size_t smem, int *nclusters)
     return cudaOccupancyMaxActiveClusters(nclusters, (void *)k_sweep, &cfg);
 }
 
-inline cudaError_t launch_sweep_cluster(unsigned nc, int cc, size_t smem, cudaStream_t st,
+/* nclus clusters of cc CTAs: the first ncoop advance one chain each, the
+ * others run up to cc of the remaining chains, one per CTA. */
+inline cudaError_t launch_sweep_cluster(unsigned nclus, int cc, size_t smem, cudaStream_t st,
                                         DqmcChainDev *c, const DqmcModelDev *m, int flags,
-                                        int nsweeps, const int *order)
+                                        int nsweeps, const int *order, int ncoop, int nchains)
 {
     cudaLaunchAttribute at[1];
-    cudaLaunchConfig_t cfg = cluster_config(nc, cc, smem, st, at);
-    return cudaLaunchKernelEx(&cfg, k_sweep, c, m, flags, nsweeps, order);
+    cudaLaunchConfig_t cfg = cluster_config(nclus, cc, smem, st, at);
+    return cudaLaunchKernelEx(&cfg, k_sweep, c, m, flags, nsweeps, order, ncoop, nchains);
 }
 
 inline void launch_measure(unsigned nc, size_t msmem, cudaStream_t st, DqmcChainDev *c,

@@ -42,7 +42,7 @@ class Desc(C.Structure):
                 ("delay_rank", C.c_int), ("drift", C.c_int),
                 ("ctas_per_sm", C.c_int), ("sweep_order", C.c_int), ("green_rebuild", C.c_int),
                 ("flush_pairs", C.c_int), ("udv_diag", C.c_int), ("green_log", C.c_int),
-                ("chain_ctas", C.c_int), ("reserved", C.c_int)]
+                ("chain_ctas", C.c_int), ("cluster_chains", C.c_int)]
 
 
 class Counters(C.Structure):
@@ -92,7 +92,8 @@ def lib():
     L.dqmc_sweep_measure.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.dqmc_synchronize.argtypes = [C.c_void_p]
     L.dqmc_chain_count.argtypes = [C.c_void_p]
-    L.dqmc_engine_residency.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.dqmc_engine_residency.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int)]
     L.dqmc_read_green.argtypes = [C.c_void_p, C.c_int, _dp]
     L.dqmc_read_field.argtypes = [C.c_void_p, C.c_int, _bp]
     L.dqmc_write_field.argtypes = [C.c_void_p, C.c_int, _bp]
@@ -210,7 +211,7 @@ class Engine:
     def __init__(self, device=0, precision=PREC_FP64, delay_rank=0,
                  drift=DRIFT_STAB, ctas_per_sm=0, sweep_order=SWEEP_FORWARD,
                  green_rebuild=REBUILD_COMBINE, flush_pairs=PAIRS_AUTO, udv_diag=0,
-                 green_log=0, chain_ctas=0):
+                 green_log=0, chain_ctas=0, cluster_chains=0):
         L = lib()
         d = Desc()
         L.dqmc_desc_default(C.byref(d))
@@ -222,6 +223,7 @@ class Engine:
         d.udv_diag = udv_diag
         d.green_log = green_log
         d.chain_ctas = chain_ctas
+        d.cluster_chains = cluster_chains
         self.green_log_cap = green_log
         self.h = L.dqmc_engine_create(C.byref(d))
         if not self.h:
@@ -384,10 +386,12 @@ class Engine:
         return ms.value
 
     def residency(self):
-        """(chains per SM, CTAs per chain) of the sweep kernel, as prepared."""
-        a, b = C.c_int(), C.c_int()
-        _check(lib().dqmc_engine_residency(self.h, C.byref(a), C.byref(b)), "residency")
-        return a.value, b.value
+        """(chains per SM, cluster size, chains on a cluster each) of the
+        sweep kernel, as prepared."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().dqmc_engine_residency(self.h, C.byref(a), C.byref(b), C.byref(c)),
+               "residency")
+        return a.value, b.value, c.value
 
     def clear_bins(self):
         _check(lib().dqmc_clear_bins(self.h), "clear_bins")

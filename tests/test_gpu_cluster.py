@@ -140,10 +140,22 @@ def test_cluster_size_chosen_automatically():
         r = e.residency()
         e.close()
         return r
-    per_sm, cc = residency(16, 1)
-    assert per_sm == 1 and cc > 1
-    assert residency(16, 1, chain_ctas=1) == (1, 1)
+    per_sm, cc, ncoop = residency(16, 1)
+    assert per_sm == 1 and cc > 1 and ncoop == 1
+    assert residency(16, 1, chain_ctas=1)[:2] == (1, 1)
     assert residency(16, 1, precision=dq.PREC_MIXED)[1] == cc
-    assert residency(8, 1) == (1, 1)
-    per_sm, cc4 = residency(16, 8)
-    assert per_sm == 1 and 1 < cc4 <= cc
+    assert residency(8, 1)[:2] == (1, 1)
+    per_sm, cc8, ncoop8 = residency(16, 8)
+    assert per_sm == 1 and 1 < cc8 <= cc and ncoop8 == 8
+
+
+def test_cluster_and_packed_chains_in_one_launch():
+    """cluster_chains: the two most expensive of six uneven chains on a
+    four-CTA cluster each, the other four packed one per CTA in the same
+    launch; everything equal to one CTA per chain."""
+    lats = [(4, 4, None), (6, 6, None), (8, 8, None), (10, 10, None), (12, 12, None),
+            (16, 16, None)]
+    run_pair(lats, 16, 8, [1, 2, 3, 4, 5, 6], 4, cluster_chains=2)
+    e = build(lats, 16, 8, [1, 2, 3, 4, 5, 6], 4, cluster_chains=2)
+    assert e.residency() == (1, 4, 2)
+    e.close()
