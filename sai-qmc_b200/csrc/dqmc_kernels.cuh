@@ -152,34 +152,31 @@ __device__ __noinline__ void flush_zy(int n, int i0, int m, int mA, const double
                 if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = two ? z[u] : z[u] * facs[p0 + u];
         }
     }
-    for (int j = lo + tid; j < hi; j += NT) {
-        double y[KB];
+    /* Ys_B: a warp per column j, lane p its entry p, lane q loading row
+     * i0 + alist[q] of column j (one coalesced segment of the column) and
+     * handing it to the other lanes by shuffles; each entry sums over q in
+     * the order of the row-per-thread Zs loop above.  YS_COLS columns per
+     * warp at a time for independent FMA chains. */
+    constexpr int YS_COLS = 8;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int m8 = (m + 7) & ~7, mA8 = (mA + 7) & ~7;
+    const int rq = i0 + alist[lane < m ? lane : 0];
+    for (int j0 = lo + warp * YS_COLS; j0 < hi; j0 += NW * YS_COLS) {
+        double yv[YS_COLS], z[YS_COLS];
 #pragma unroll
-        for (int q = 0; q < KB; ++q)
-            y[q] = q < m ? G[(i0 + alist[q]) + (size_t)j * n] : 0.0;
-        for (int p0 = 0; p0 < m; p0 += 8) {
-            double z[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) z[u] = 0.0;
-#pragma unroll
-            for (int q0 = 0; q0 < KB; q0 += 8) {
-                if (q0 < m) {
-#pragma unroll
-                    for (int q = q0; q < q0 + 8; ++q) {
-#pragma unroll
-                        for (int u = 0; u < 8; u += 2) {
-                            const double2 t =
-                                *reinterpret_cast<const double2 *>(TvP + q * LT + p0 + u);
-                            z[u] = fma(t.x, y[q], z[u]);
-                            z[u + 1] = fma(t.y, y[q], z[u + 1]);
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+        for (int c = 0; c < YS_COLS; ++c) {
+            const int j = j0 + c;
+            yv[c] = (j < hi && lane < m) ? G[rq + (size_t)j * n] : 0.0;
+            z[c] = 0.0;
         }
+        for (int q = 0; q < m8; ++q) {
+            const double t = TvP[q * LT + lane];
+#pragma unroll
+            for (int c = 0; c < YS_COLS; ++c) z[c] = fma(t, __shfl_sync(FULL, yv[c], q), z[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < YS_COLS; ++c)
+            if (j0 + c < hi && lane < m) YsB[lane + (size_t)(j0 + c) * ldy] = z[c];
     }
     if (two) {
         /* each thread re-reads only what it wrote in pass 1 */
@@ -212,34 +209,23 @@ __device__ __noinline__ void flush_zy(int n, int i0, int m, int mA, const double
                     if (p0 + u < m) ZsB[i + (size_t)(p0 + u) * n] = z[u] * facs[p0 + u];
             }
         }
-        for (int j = lo + tid; j < hi; j += NT) {
-            double ya[KB];
+        for (int j0 = lo + warp * YS_COLS; j0 < hi; j0 += NW * YS_COLS) {
+            double ya[YS_COLS], z[YS_COLS];
 #pragma unroll
-            for (int k = 0; k < KB; ++k) ya[k] = k < mA ? Ys[k + (size_t)j * ldy] : 0.0;
-            for (int p0 = 0; p0 < m; p0 += 8) {
-                double z[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    z[u] = p0 + u < m ? YsB[(p0 + u) + (size_t)j * ldy] : 0.0;
-#pragma unroll
-                for (int k0 = 0; k0 < KB; k0 += 8) {
-                    if (k0 < mA) {
-#pragma unroll
-                        for (int k = k0; k < k0 + 8; ++k) {
-#pragma unroll
-                            for (int u = 0; u < 8; u += 2) {
-                                const double2 t =
-                                    *reinterpret_cast<const double2 *>(PaT + k * LT + p0 + u);
-                                z[u] = fma(t.x, ya[k], z[u]);
-                                z[u + 1] = fma(t.y, ya[k], z[u + 1]);
-                            }
-                        }
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (p0 + u < m) YsB[(p0 + u) + (size_t)j * ldy] = z[u];
+            for (int c = 0; c < YS_COLS; ++c) {
+                const int j = j0 + c;
+                ya[c] = (j < hi && lane < mA) ? Ys[lane + (size_t)j * ldy] : 0.0;
+                z[c] = (j < hi && lane < m) ? YsB[lane + (size_t)j * ldy] : 0.0;
             }
+            for (int k = 0; k < mA8; ++k) {
+                const double t = PaT[k * LT + lane];
+#pragma unroll
+                for (int c = 0; c < YS_COLS; ++c)
+                    z[c] = fma(t, __shfl_sync(FULL, ya[c], k), z[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < YS_COLS; ++c)
+                if (j0 + c < hi && lane < m) YsB[lane + (size_t)(j0 + c) * ldy] = z[c];
         }
     }
     if (s.cl.c > 1)
