@@ -828,7 +828,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
      * (the ncoop most expensive chains in launch order) or runs cc of the
      * other chains, one per CTA.  Explicit: chain_ctas > 1, cluster_chains
      * of them (0 = all).  Automatic (chain_ctas = 0) for batches of fewer
-     * chains than SMs whose largest lattice has n >= 128: the (cc, ncoop)
+     * chains than SMs whose largest lattice has n >= 128: the (cc in 2..16,
+     * ncoop)
      * whose slowest chain is predicted fastest, every cluster resident at
      * once (a second wave of clusters costs more than narrower ones), by
      * chain cost n^3 L (doubled on the two-spin path) over the speedup
@@ -875,9 +876,8 @@ int dqmc_engine_prepare(dqmc_engine *e, int nbin)
             e->ncoop = k;
             e->nclus = tot;
         } else if (want == 0 && e->per_sm == 1 && maxn >= 128) {
-            static const int sizes[] = {16, 12, 8, 6, 4, 3, 2};
             double best = w.empty() ? 0.0 : w[0];
-            for (int cc : sizes) {
+            for (int cc = DQMC_MAX_CHAIN_CTAS; cc >= 2; --cc) {
                 int fit = 0;
                 if (dq::cluster_fit(cc, e->smem, &fit) != cudaSuccess) {
                     cudaGetLastError();

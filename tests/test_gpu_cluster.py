@@ -51,12 +51,12 @@ def run_pair(lats, L, stab, seeds, ctas, sweeps=2, **kw):
     cl.close()
 
 
-@pytest.mark.parametrize("ctas", [2, 4, 8])
+@pytest.mark.parametrize("ctas", [2, 3, 4, 8])
 def test_cluster_equals_one_cta_8x8(ctas):
     run_pair([(8, 8, None)], 40, 10, [7], ctas)
 
 
-@pytest.mark.parametrize("ctas", [4, 8, 16])
+@pytest.mark.parametrize("ctas", [4, 8, 12, 16])
 def test_cluster_equals_one_cta_16x16(ctas):
     """n = 256: 128x128 or 64x64 tiles by share, paired site blocks."""
     run_pair([(16, 16, None)], 16, 8, [11], ctas)
