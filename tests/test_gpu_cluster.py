@@ -159,3 +159,28 @@ def test_cluster_and_packed_chains_in_one_launch():
     e = build(lats, 16, 8, [1, 2, 3, 4, 5, 6], 4, cluster_chains=2)
     assert e.residency() == (1, 4, 2)
     e.close()
+
+
+@pytest.mark.parametrize("prec", [dq.PREC_FP64, dq.PREC_MIXED])
+def test_cluster_chain_failure_stops_only_that_chain(prec):
+    """A chain on a cluster whose G is corrupted from the host stops at its
+    first stabilization point (rank 0 leaves the sweep and releases the other
+    ranks); its batch-mates, also on clusters, equal a clean run."""
+    lats, seeds = [(16, 16, None)] * 3, [3, 4, 5]
+    clean = build(lats, 16, 8, seeds, 4, precision=prec)
+    hit = build(lats, 16, 8, seeds, 4, precision=prec)
+    G = hit.green(1)
+    G[2, 3] = np.nan
+    hit.write_green(1, G)
+    clean.sweep(2)
+    hit.sweep(2)
+    c = hit.counters(1)
+    assert c["status"] & 1 and c["sign"] == 0.0 and c["sweeps"] == 0
+    for k in (0, 2):
+        np.testing.assert_array_equal(hit.field(k), clean.field(k))
+        assert hit.counters(k)["status"] == 0
+        assert np.array_equal(hit.green(k), clean.green(k))
+    hit.sweep(1)                                   # the frozen chain stays frozen
+    assert hit.counters(1)["attempts"] == c["attempts"]
+    clean.close()
+    hit.close()
