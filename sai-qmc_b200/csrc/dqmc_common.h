@@ -106,9 +106,10 @@ typedef struct {
 /* per-chain global staging for the other ranks of a chain's cluster: a site
  * block's flush operands (four DQMC_MAX_KB x (DQMC_MAX_KB + 2) blocks, the
  * DQMC_MAX_KB factors and the accepted list), then the pre-pivot's column
- * norms (DQMC_MAX_N)                                                     */
+ * norms (DQMC_MAX_N), then each rank's reflector count and flags of a QR
+ * factorization (two ints per rank)                                      */
 #define DQMC_CL_FLUSH_DOUBLES (4 * DQMC_MAX_KB * (DQMC_MAX_KB + 2) + 2 * DQMC_MAX_KB)
-#define DQMC_CL_STAGE_DOUBLES (DQMC_CL_FLUSH_DOUBLES + DQMC_MAX_N)
+#define DQMC_CL_STAGE_DOUBLES (DQMC_CL_FLUSH_DOUBLES + DQMC_MAX_N + DQMC_MAX_CHAIN_CTAS)
 
 typedef struct {
     int model, n, L, stab, M, kb;

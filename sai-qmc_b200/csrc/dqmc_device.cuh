@@ -654,7 +654,8 @@ enum {
     CL_ZY,          /* flush_zy: row and column ranges                 */
     CL_PREPIV,      /* prepivot: column norms and the gather by columns */
     CL_WSPLIT,      /* wrap_green_split: lines of each split, tiles     */
-    CL_FSPLIT       /* flush_split: lines of each split, tiles          */
+    CL_FSPLIT,      /* flush_split: lines of each split, tiles          */
+    CL_QRF          /* qr_factor_cl: a column block per rank            */
 };
 
 __device__ __forceinline__ void cl_sync()
@@ -1616,10 +1617,75 @@ __device__ __forceinline__ void qr_panels(QrSm &q, int n, const double *A, const
     }
 }
 
+/* qr_factor_sm as a split command of a cluster per chain (no more column
+ * blocks than ranks): column block b belongs to rank b, which keeps it in
+ * its shared memory from its load to its store.  At step b the owner of
+ * block b factors it (every earlier panel is already applied) and stores
+ * it; after the barrier every owner of a later block applies block b's
+ * panels to its own.  Each block thus sees the one-CTA code's sequence of
+ * panel applications (only their grouping into qr_panels calls differs,
+ * which moves no arithmetic), so A, tw and the reflector count are the same
+ * to the bit; the critical path holds one block's applications per step
+ * instead of all earlier panels.  Counts and flags of the other ranks come
+ * back through the chain's staging area. */
+__device__ __noinline__ int qr_factor_cl(int n, double *A, double *tw, Smem &s, int *flag)
+{
+    cl_post(s, CL_QRF, A, tw, nullptr, nullptr, nullptr, nullptr, n, 0, 0);
+    QrSm &q = s.q;
+    const int ld = q.ld, cb = q.cb, r = s.cl.r;
+    const int nblk = (n + cb - 1) / cb;
+    const bool own = r < nblk;
+    const int jb = r * cb, nc = own ? min(cb, n - jb) : 0;
+    int nontrivial = 0;
+    if (own) qr_load_cols(q, n, A, jb, nc);
+    for (int b = 0; b < nblk; ++b) {
+        if (own && r == b) {
+            for (int pc = 0; pc < nc; pc += 16) {
+                const int j0 = jb + pc, m = n - j0, nb = min(16, m);
+                double *Xp = q.X + j0 + (size_t)pc * ld;
+                if (m <= NT)
+                    nontrivial += qr_panel<1>(q, Xp, m, nb, flag);
+                else if (m <= 2 * NT)
+                    nontrivial += qr_panel<2>(q, Xp, m, nb, flag);
+                else
+                    nontrivial += qr_panel<3>(q, Xp, m, nb, flag);
+                double *twp = tw + (size_t)(j0 / 16) * 256;
+                for (int e = threadIdx.x; e < 256; e += NT) twp[e] = q.T[e];
+                if (pc + 16 < nc) qr_apply_sm(q, Xp + (size_t)16 * ld, m, nc - pc - 16, true);
+            }
+            qr_store_cols(q, n, A, jb, nc);
+            __syncthreads();
+        }
+        cl_sync();
+        if (own && r > b)
+            qr_panels(q, n, A, tw, b * cb, 16, cb / 16,
+                      [&](int p0) { qr_apply_sm(q, q.X + p0, n - p0, nc, true); });
+    }
+    int *rep = reinterpret_cast<int *>(s.stage + DQMC_CL_FLUSH_DOUBLES + DQMC_MAX_N);
+    if (own && threadIdx.x == 0) {
+        rep[2 * r] = nontrivial;
+        rep[2 * r + 1] = *flag;
+    }
+    cl_sync();
+    if (r == 0) {
+        int tot = 0, bits = 0;
+        for (int k = 0; k < nblk; ++k) {
+            tot += rep[2 * k];
+            bits |= rep[2 * k + 1];
+        }
+        nontrivial = tot;
+        if (bits && threadIdx.x == 0) raise_flag(flag, bits);
+    }
+    __syncthreads();
+    return nontrivial;
+}
+
 __device__ __noinline__ int qr_factor_sm(int n, double *A, double *tw, Smem &s, int *flag)
 {
     QrSm &q = s.q;
     const int ld = q.ld, cb = q.cb;
+    if (s.cl.c > 1 && s.cl.r == 0 && n > cb && (n + cb - 1) / cb <= s.cl.c)
+        return qr_factor_cl(n, A, tw, s, flag);
     int nontrivial = 0;
     for (int jb = 0; jb < n; jb += cb) {
         const int nc = min(cb, n - jb);

@@ -278,6 +278,7 @@ __device__ __forceinline__ void g_update(int n, int mt, double *G, const double 
  * rank 0 never rewrites it while it is being read. */
 __device__ __noinline__ void cl_serve(Smem &s)
 {
+    __shared__ int sflag;   /* flags this rank raises in a command */
     for (;;) {
         cl_sync();
         const DqmcClCmd *c = s.cmd;
@@ -318,6 +319,11 @@ __device__ __noinline__ void cl_serve(Smem &s)
             break;
         case CL_UGEMM:
             udv_gemm(i1, i0, (const double *)p0, (const double *)p1, (double *)p2, s);
+            break;
+        case CL_QRF:
+            if (threadIdx.x == 0) sflag = 0;
+            __syncthreads();
+            qr_factor_cl(i0, (double *)p0, (double *)p1, s, &sflag);
             break;
         case CL_PREPIV:
             prepivot_cl(i0, (const double *)p0, (double *)p1, s, nullptr);
