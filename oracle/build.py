@@ -5,7 +5,8 @@ Two artefacts:
 * ``oracle/liboracle.so`` -- the plain-C restatement of the reference's BSS
   sweep in ``oracle/oracle.c`` (no external libraries; built everywhere).
 * ``oracle/_ref/`` -- the UNMODIFIED reference compiled from its own sources
-  where they lie (``$SAIQMC_REF``, default ``/root/reference``), linked
+  where they lie (``$SAIQMC_REF``, else a ``reference`` directory beside
+  the repository), linked
   against the OpenBLAS 0.3.15 that ships inside the opencv wheel of this
   image (the reference calls Fortran BLAS/LAPACK symbols, linalg.c:27-42):
     - ``libdqmcref.so``: reference src/*.c minus main.c + ``ref_shim.c``

@@ -1,7 +1,8 @@
 """Generate the golden parity fixtures from the UNMODIFIED reference.
 
-Run in a container where the reference sources exist (``$SAIQMC_REF``,
-default /root/reference): ``python tests/golden/make_golden.py``.  It
+Run in a container where the reference sources exist (``$SAIQMC_REF``, else
+a ``reference`` directory beside the repository):
+``python tests/golden/make_golden.py``.  It
 builds oracle/_ref (oracle/build.py), drives the reference engine through
 oracle/ref_shim.c and writes small .npz files next to this script.  The
 reference's own UDV fixtures (tests/fixtures/udv_phase6a_*.txt, read here as
