@@ -184,3 +184,10 @@ def test_cluster_chain_failure_stops_only_that_chain(prec):
     assert hit.counters(1)["attempts"] == c["attempts"]
     clean.close()
     hit.close()
+
+
+@pytest.mark.parametrize("rebuild", [dq.REBUILD_TWO_SIDED, dq.REBUILD_CENTERED])
+def test_cluster_two_sided_rebuild(rebuild):
+    """G from the two boundary factors (its QR solve and triangular solves run
+    as cluster commands) with UDV scale records on."""
+    run_pair([(10, 10, None)], 24, 6, [5], 4, sweeps=3, green_rebuild=rebuild, udv_diag=1)
