@@ -704,8 +704,9 @@ def run_gpu_arm(args):
             # one chain: a thread-block cluster per chain (automatic size)
             # and, for comparison, one CTA per chain; same trajectory
             single = {}
-            for key, cc in (("cluster", 0), ("one_cta", 1)):
-                e1 = make_engine(dq, 1, 0, precision, chain_ctas=cc)
+            for key, cc, prec in (("cluster", 0, precision), ("one_cta", 1, precision),
+                                  ("mixed_cluster", 0, dq.PREC_MIXED)):
+                e1 = make_engine(dq, 1, 0, prec, chain_ctas=cc)
                 e1.prepare(1)
                 e1.sweep(1)
                 e1.sync()
@@ -718,7 +719,9 @@ def run_gpu_arm(args):
             line["single_chain"] = {"value": N_SITES * L_SLICES / (t1 * 1e-3), "unit": UNIT,
                                     "ms_per_sweep": t1, "chain_ctas": cc1,
                                     "one_cta_ms_per_sweep": single["one_cta"][0],
-                                    "over_one_cta": single["one_cta"][0] / t1}
+                                    "over_one_cta": single["one_cta"][0] / t1,
+                                    "mixed_ms_per_sweep": single["mixed_cluster"][0],
+                                    "mixed_chain_ctas": single["mixed_cluster"][1]}
         if e2e is not None:
             line["e2e"] = e2e
         if not args.no_cpu_baseline and world == 1:
